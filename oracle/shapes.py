@@ -1,0 +1,247 @@
+"""Oracle restatement of the plane-wave grids and the shape Fourier transforms.
+
+Follows ``code/source/8_band/basis_set.c:23-90``,
+``code/source/8_band/characteristic_function_fourier.c:58-1411`` and
+``code/source/8_band/characteristic_function_fourier_integrals.c:28-153``
+(test infrastructure).
+
+Shapes implemented: 0 cuboid, 4 lens (hemi-ellipsoid), 5 pyramid, 6 truncated
+pyramid, 16 N-sided prism, 17 quantum well.  Every function is scalar and is
+vectorised with ``numpy.vectorize`` by ``chi_table``; the oracle is meant for
+small grids.
+"""
+
+import cmath
+import math
+
+import numpy as np
+from scipy.special import j0, j1
+
+EPS = 1.0e-08
+
+
+def basis_grid(n_T, L):
+    """G_i = (2 pi / L)(0.5 (1 - n_T) + i), i < n_T (basis_set.c:62-85)."""
+    i = np.arange(n_T, dtype=np.float64)
+    return ((2.0 * math.pi) / L) * (0.5 * (1.0 - float(n_T)) + i)
+
+
+def make_basis(N, L, K=(0.0, 0.0, 0.0)):
+    """Basis with N plane waves per axis and grids of length 2N-1 (8_band_main.c:206-227)."""
+    b = {"N": tuple(int(n) for n in N), "N_T": tuple(2 * int(n) - 1 for n in N), "K": tuple(K)}
+    b["G"] = tuple(basis_grid(2 * int(n) - 1, l) for n, l in zip(N, L))
+    return b
+
+
+def sinc_pi(x):
+    """gsl_sf_sinc: sin(pi x)/(pi x)."""
+    return float(np.sinc(x))
+
+
+# Gauss-Legendre rule for I_J0 (see i_j0)
+_GL_X, _GL_W = np.polynomial.legendre.leggauss(96)
+_GL_X = 0.5 * (_GL_X + 1.0)
+_GL_W = 0.5 * _GL_W
+
+
+def i_j0(alpha, beta):
+    """I_J0(alpha, beta) = int_0^1 x cos(alpha sqrt(1-x^2)) J0(beta x) dx
+    (characteristic_function_fourier_integrals.c:107-153, GSL QAG key 6 with
+    EPS_ABS = EPS_REL = 1e-4).  cos(alpha sqrt(1-x^2)) is a power series in
+    (1 - x^2), so the integrand is entire and QAG's first 61-point Kronrod pass
+    already converges to rounding for the |alpha|, |beta| <= ~40 met by these
+    grids; a 96-point Gauss-Legendre rule gives the same value."""
+    x = _GL_X
+    return float(np.sum(_GL_W * x * np.cos(alpha * np.sqrt(1.0 - x * x)) * j0(beta * x)))
+
+
+def i_e0(a, G):
+    """characteristic_function_fourier_integrals.c:28-47."""
+    if abs(G) < EPS:
+        return complex(a)
+    return (cmath.exp(1j * G * a) - 1.0) / (1j * G)
+
+
+def pyramid_segment(Gx0, Gy0, Gz0, idx_side, N_side, g):
+    """characteristic_function_fourier.c:1112-1296."""
+    L1, L2, L3 = g["L1"], g["L2"], g["L3"]
+    if N_side == 0:
+        if idx_side in (0, 2):
+            alpha = math.atan(L2 / L1)
+        else:
+            alpha = math.atan(L1 / L2)
+    else:
+        alpha = math.pi / float(N_side)
+    if N_side == 0 and idx_side in (0, 2):
+        x0, y0 = L1, L2
+    elif N_side == 0 and idx_side in (1, 3):
+        x0, y0 = L2, L1
+    else:
+        x0, y0 = L1, math.tan(alpha) * L1
+    h = L3 if N_side == 0 else L2
+    ang = 2.0 * alpha * float(idx_side)
+    Gx = math.cos(ang) * Gx0 + math.sin(ang) * Gy0
+    Gy = -1.0 * math.sin(ang) * Gx0 + math.cos(ang) * Gy0
+    Gz = Gz0
+    G_mag = math.sqrt(Gx ** 2 + Gy ** 2 + Gz ** 2)
+    I = 1j
+    ex = cmath.exp
+    if abs(G_mag) < EPS:
+        return (x0 * y0 * h) / 3.0
+    if abs(Gx) < EPS and abs(Gy) < EPS:
+        return ((I * 2.0 * y0 * x0) / Gz) * ((1.0 - I * Gz * h - ex(-1.0 * I * Gz * h)) / (Gz * Gz * h * h) - 0.5)
+    if abs(Gx) < EPS and abs(Gz) < EPS:
+        return ((2.0 * h * x0) / (Gy * Gy * y0)) * (1.0 - math.sin(Gy * y0) / (Gy * y0))
+    if abs(Gy) < EPS and abs(Gz) < EPS:
+        return ((2.0 * h * y0) / (Gx * Gx * x0)) * (-1.0 - ex(-1.0 * I * Gx * x0) - (2.0 * I) / (Gx * x0)
+                                                   + 2.0 * I * ex(-1.0 * I * Gx * x0) / (Gx * x0))
+    if abs(Gx) < EPS:
+        c = 2.0 * (math.cos(Gy * y0) - 1.0) / (Gy * y0)
+        pre = (-1.0 * I * x0) / (Gz * Gy)
+        if abs(Gy * y0 - Gz * h) < EPS:
+            return pre * (ex(-1.0 * I * Gz * h) * (-1.0 * I + (ex(I * (Gy * y0 + Gz * h)) - 1.0) / (Gy * y0 + Gz * h)) - c)
+        if abs(Gy * y0 + Gz * h) < EPS:
+            return pre * (ex(-1.0 * I * Gz * h) * ((ex(-1.0 * I * (Gy * y0 - Gz * h)) - 1.0) / (Gy * y0 - Gz * h) + I) - c)
+        return pre * (ex(-1.0 * I * Gz * h) * ((ex(-1.0 * I * (Gy * y0 - Gz * h)) - 1.0) / (Gy * y0 - Gz * h)
+                                               + (ex(I * (Gy * y0 + Gz * h)) - 1.0) / (Gy * y0 + Gz * h)) - c)
+    if abs(Gy) < EPS:
+        pre = (2.0 * I * y0) / (Gz * x0)
+        t2 = (ex(-1.0 * I * Gx * x0) * (1.0 + I * Gx * x0) - 1.0) / (Gx * Gx)
+        if abs(Gx - (Gz * h) / x0) < EPS:
+            return pre * (0.5 * ex(-1.0 * I * Gz * h) * x0 * x0 - t2)
+        return pre * (ex(-1.0 * I * Gz * h) * (ex(-1.0 * I * (Gx * x0 - Gz * h)) * (1.0 + I * (Gx * x0 - Gz * h)) - 1.0)
+                      / (Gx - (Gz * h) / x0) ** 2 - t2)
+    if abs(Gz) < EPS:
+        ap = Gx + (Gy * y0) / x0
+        am = Gx - (Gy * y0) / x0
+        if abs(Gx - (Gy * y0) / x0) < EPS:
+            return (h / Gy) * (1.0 / ap - (I / (x0 * ap ** 2)) * (ex(-1.0 * I * x0 * ap) - 1.0) - 0.5 * I * x0)
+        if abs(Gx + (Gy * y0) / x0) < EPS:
+            return (h / Gy) * (-1.0 / am + (I / (x0 * am ** 2)) * (ex(-1.0 * I * x0 * am) - 1.0) + 0.5 * I * x0)
+        return (h / Gy) * (1.0 / ap - 1.0 / am - (I / (x0 * ap ** 2)) * (ex(-1.0 * I * x0 * ap) - 1.0)
+                           + (I / (x0 * am ** 2)) * (ex(-1.0 * I * x0 * am) - 1.0))
+    e = ex(-1.0 * I * Gz * h)
+    return (-1.0 / (Gy * Gz)) * (i_e0(x0, -1.0 * Gx - (Gy * y0) / x0 + (Gz * h) / x0) * e
+                                 - i_e0(x0, -1.0 * Gx + (Gy * y0) / x0 + (Gz * h) / x0) * e
+                                 - i_e0(x0, -1.0 * Gx - (Gy * y0) / x0)
+                                 + i_e0(x0, -1.0 * Gx + (Gy * y0) / x0))
+
+
+def prism_segment(Gx0, Gy0, Gz0, idx_side, N_side, g):
+    """characteristic_function_fourier.c:1298-1411."""
+    alpha = math.pi / float(N_side)
+    x0, h = g["L1"], g["L2"]
+    ang = (2.0 * math.pi * float(idx_side)) / N_side
+    Gx = math.cos(ang) * Gx0 + math.sin(ang) * Gy0
+    Gy = -1.0 * math.sin(ang) * Gx0 + math.cos(ang) * Gy0
+    Gz = Gz0
+    G_mag = math.sqrt(Gx ** 2 + Gy ** 2 + Gz ** 2)
+    I = 1j
+    ex = cmath.exp
+    ta = math.tan(alpha)
+    if abs(G_mag) < EPS:
+        return x0 * x0 * h * ta
+    if abs(Gx) < EPS and abs(Gy) < EPS:
+        return 2.0 * x0 * x0 * ta * math.sin(0.5 * Gz * h) / Gz
+    if abs(Gx) < EPS and abs(Gz) < EPS:
+        return (2.0 * h / (Gy * Gy * ta)) * (1.0 - math.cos(Gy * x0 * ta))
+    if abs(Gy) < EPS and abs(Gz) < EPS:
+        return (2.0 * h * ta / Gx) * (1.0 * I * x0 * ex(-1.0 * I * Gx * x0) + (1.0 / Gx) * (ex(-1.0 * I * Gx * x0) - 1.0))
+    if abs(Gx) < EPS:
+        return (4.0 * math.sin(0.5 * Gz * h) / (Gy * Gy * Gz * ta)) * (1.0 - math.cos(Gy * x0 * ta))
+    if abs(Gy) < EPS:
+        return (4.0 * math.sin(0.5 * Gz * h) * ta / (Gz * Gx)) * (1.0 * I * x0 * ex(-1.0 * I * Gx * x0)
+                                                                  + (1.0 / Gx) * (ex(-1.0 * I * Gx * x0) - 1.0))
+    if abs(Gz) < EPS:
+        pre = h / Gy
+    else:
+        pre = (2.0 / (Gy * Gz)) * math.sin(0.5 * Gz * h)
+    if abs(Gy * ta + Gx) < EPS:
+        return pre * (1.0 * I * x0 - (1.0 / (-Gy * ta + Gx)) * (1.0 - ex(1.0 * I * Gy * x0 * ta - 1.0 * I * Gx * x0)))
+    if abs(-Gy * ta + Gx) < EPS:
+        return pre * ((1.0 / (Gy * ta + Gx)) * (1.0 - ex(-1.0 * I * Gy * x0 * ta - 1.0 * I * Gx * x0)) - 1.0 * I * x0)
+    return pre * ((1.0 / (Gy * ta + Gx)) * (1.0 - ex(-1.0 * I * Gy * x0 * ta - 1.0 * I * Gx * x0))
+                  - (1.0 / (-Gy * ta + Gx)) * (1.0 - ex(1.0 * I * Gy * x0 * ta - 1.0 * I * Gx * x0)))
+
+
+def chi(Gx0, Gy0, Gz0, geo, idx, cell, softening=0, sigma=0.0):
+    """characteristic_function_fourier.c:58-1110 for one wave vector.
+
+    ``cell`` is the supercell_type argument: 0 electronic-structure cell,
+    1/2 strain cell, 3 Coulomb cell (selects the volume normalisation)."""
+    g = geo[idx]
+    g0 = geo[0]
+    phase = cmath.exp(-1.0j * (Gx0 * g["Ox"] + Gy0 * g["Oy"] + Gz0 * g["Oz"]))
+    if cell == 3:
+        r = phase / (g0["CL1"] * g0["CL2"] * g0["CL3"])
+    elif cell == 0 or idx == 0:
+        r = phase / (g0["L1"] * g0["L2"] * g0["L3"])
+    else:
+        r = phase / (g0["SL1"] * g0["SL2"] * g0["SL3"])
+    sa, ca = math.sin(math.pi * g["alpha"] / 180), math.cos(math.pi * g["alpha"] / 180)
+    sb, cb = math.sin(math.pi * g["beta"] / 180), math.cos(math.pi * g["beta"] / 180)
+    sg, cg = math.sin(math.pi * g["gamma"] / 180), math.cos(math.pi * g["gamma"] / 180)
+    Gx = ((cb * ca * cg) - (sa * sg)) * Gx0 + ((cg * cb * sa) + (sg * ca)) * Gy0 + (-sb * cg) * Gz0
+    Gy = ((cb * -ca * sg) - (sa * cg)) * Gx0 + ((-sg * cb * sa) + (cg * ca)) * Gy0 + (sb * sg) * Gz0
+    Gz = (sb * ca) * Gx0 + (sa * sb) * Gy0 + (cb) * Gz0
+    if softening != 0:
+        r *= math.exp(-0.5 * sigma ** 2 * (Gx ** 2 + Gy ** 2 + Gz ** 2))
+    shape = g["shape"]
+    L1, L2, L3, L4 = g["L1"], g["L2"], g["L3"], g["L4"]
+    if shape == 0:
+        r *= (L1 * sinc_pi((0.5 * Gx * L1) / math.pi) * L2 * sinc_pi((0.5 * Gy * L2) / math.pi)
+              * L3 * sinc_pi((0.5 * Gz * L3) / math.pi))
+    elif shape == 4:
+        G_mag = math.sqrt((Gx * L1) ** 2 + (Gy * L2) ** 2 + (Gz * L3) ** 2)
+        G_par = math.sqrt((Gx * L1) ** 2 + (Gy * L2) ** 2)
+        if abs(G_mag) < EPS:
+            r *= (2.0 * math.pi * L1 * L2 * L3) / 3.0
+        else:
+            sphere = (2.0 * math.pi * L1 * L2 * L3 * (math.sin(G_mag) - G_mag * math.cos(G_mag))) / G_mag ** 3
+            if abs(G_par) < EPS:
+                r *= sphere - (2.0 * math.pi * 1j * L1 * L2 / Gz) * (
+                    0.5 - (math.cos(Gz * L3) + Gz * L3 * math.sin(L3 * Gz) - 1.0) / (Gz * L3) ** 2)
+            elif abs(Gz) < EPS:
+                r *= sphere
+            else:
+                r *= sphere - (2.0 * math.pi * 1j * L1 * L2 / Gz) * (float(j1(G_par)) / G_par - i_j0(Gz * L3, G_par))
+    elif shape == 5:
+        r *= sum(pyramid_segment(Gx, Gy, Gz, s, 0, geo[idx]) for s in range(4))
+    elif shape == 6:
+        g2 = dict(g)
+        g2["L3"] = (L4 * L1) / (L1 - L3)
+        seg = sum(pyramid_segment(Gx, Gy, Gz, s, 0, g2) for s in range(4))
+        g2["L1"] = L3
+        g2["L2"] = (L2 * L3) / L1
+        g2["L3"] = (L4 * L3) / (L1 - L3)
+        for s in range(4):
+            seg -= cmath.exp(-1.0j * Gz * L4) * pyramid_segment(Gx, Gy, Gz, s, 0, g2)
+        r *= seg
+    elif shape == 16:
+        n = int(round(0.1 * L3))
+        r *= sum(prism_segment(Gx, Gy, Gz, s, n, g) for s in range(n))
+    elif shape == 17:
+        d = int(round(0.1 * L1))
+        if cell == 0:
+            dims = (g0["L1"], g0["L2"], g0["L3"])
+        else:
+            dims = (g0["SL1"], g0["SL2"], g0["SL3"])
+        lens = list(dims)
+        lens[d] = L2
+        r *= (lens[0] * sinc_pi((0.5 * Gx * lens[0]) / math.pi) * lens[1] * sinc_pi((0.5 * Gy * lens[1]) / math.pi)
+              * lens[2] * sinc_pi((0.5 * Gz * lens[2]) / math.pi))
+    else:
+        raise NotImplementedError("shape %d is not in the oracle" % shape)
+    return r
+
+
+def chi_table(basis, geo, idx, cell, softening=0, sigma=0.0):
+    """chi_s on the (2N-1)^3 grid, index iz + N_zT (iy + N_yT ix)
+    (characteristic_functions_reciprocal_space.c:53-80)."""
+    Gx, Gy, Gz = basis["G"]
+    out = np.empty((len(Gx), len(Gy), len(Gz)), dtype=np.complex128)
+    for a, gx in enumerate(Gx):
+        for b, gy in enumerate(Gy):
+            for c, gz in enumerate(Gz):
+                out[a, b, c] = chi(float(gx), float(gy), float(gz), geo, idx, cell, softening, sigma)
+    return out
