@@ -1,0 +1,231 @@
+/*
+ * qudos_b200 -- B200 (sm_100a) implementation of the QUDOS plane-wave (PWEM)
+ * solve path: 8-band k.p supercell Hamiltonian assembly, partial dense
+ * Hermitian eigensolve for the states nearest the gap, and the FFT-based
+ * Coulomb matrix elements.
+ *
+ * Two layers are exported from libqdgpu.so:
+ *
+ *  1. The reference's own routines, same names, same arguments, same global
+ *     state (QUDOS code/source/8_band/8_band.h).  They run on the GPU.  The
+ *     reference's globals are defined here as weak symbols so that the
+ *     reference's 8_band_main.c, linked against this library, provides them.
+ *
+ *  2. Status-returning entry points with plain pointers and sizes (prefix
+ *     qd_), used by the driver program, the Python binding and the tests.
+ *     They never exit the process; they return QD_OK or a QD_ERR_* code and
+ *     qd_last_error_message() describes the failure.
+ *
+ * Only one GPU is used (the current CUDA device).  Calls are not re-entrant
+ * (the reference keeps global state); one call at a time per process.
+ */
+#ifndef QUDOS_B200_H
+#define QUDOS_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+typedef struct { double re, im; } qd_complex128;
+typedef struct { float re, im; } qd_complex64;
+#else
+#include <complex.h>
+typedef double _Complex qd_complex128;
+typedef float _Complex qd_complex64;
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Reference ABI types (layout identical to code/source/8_band/8_band.h)      */
+/* ------------------------------------------------------------------------- */
+#ifndef QD_NO_REFERENCE_TYPES
+/* 8_band.h:117-124 */
+struct wave_vectors {
+    int N_Gx, N_Gy, N_Gz;
+    int N_Gx_T, N_Gy_T, N_Gz_T;
+    double *Gx, *Gy, *Gz;
+    double Kx, Ky, Kz;
+};
+/* 8_band.h:126 */
+struct characteristic_functions { qd_complex128 *chi; };
+/* 8_band.h:130 */
+struct vector { double x, y, z; };
+/* 8_band.h:134-138 */
+struct strain_tensor { qd_complex128 *xx, *yy, *zz, *yz, *xz, *xy; };
+/* 8_band.h:140-144 (only the first eight tables are read by the solve path) */
+struct convolution_char_strain {
+    qd_complex128 *char_xx, *char_yy, *char_zz, *char_yz, *char_xz, *char_xy, *char_hydrostatic,
+        *char_biaxial, *xx_yz, *yy_yz, *zz_yz, *xy_xz, *yy_xz, *xx_xz, *zz_xz, *xy_yz, *zz_xy,
+        *xx_xy, *yy_xy, *xz_yz, *char_xx_yz, *char_yy_yz, *char_zz_yz, *char_xy_xz, *char_yy_xz,
+        *char_xx_xz, *char_zz_xz, *char_xy_yz, *char_zz_xy, *char_xx_xy, *char_yy_xy, *char_xz_yz;
+};
+/* 8_band.h:146-150 */
+struct piezo_potential { qd_complex128 *pz; };
+/* 8_band.h:170-174 */
+struct coulomb_matrix_element { qd_complex128 *ee, *hh, *eh_direct, *eh_exchange; };
+/* 8_band.h:190-194 */
+struct timing {
+    double char_s_grid, char_es_grid, strain_s_grid, piezo_s_grid, strain_es_grid, piezo_es_grid,
+        conv, ham_elements, ham_diag, eig, bloch, overlaps, car_loc, mme, linescan, cross_section,
+        real_3D, cme_B, cme_I, cme_total, total;
+};
+/* 8_band.h:197 */
+struct supercell_geometry {
+    int shape, embedded, material, material_type, RL1, RL2, RL3, RCL1, RCL2, RCL3;
+    double x, y, Ox, Oy, Oz, L1, L2, L3, L4, L5, SL1, SL2, SL3, CL1, CL2, CL3, alpha, beta, gamma;
+};
+/* 8_band.h:200 */
+struct material_params {
+    double a, C11, C12, C44, e14, B114, B124, B156, Eg, Dso, Ep, P, sc, g1, g2, g3, ac, av, b, d,
+        Ev_avg, E_so, E_lh, E_hh, E_cb, nr;
+};
+/* 8_band.h:209-211 */
+struct eigenstate {
+    int idx_state;
+    double E, *bloch, *probability_1, *probability_2, *probability_3, *probability_4,
+        *probability_5, *probability_6, *probability_7, *probability_8;
+    qd_complex128 *fourier, *F_1, *F_2, *F_3, *F_4, *F_5, *F_6, *F_7, *F_8;
+};
+
+/* ------------------------------------------------------------------------- */
+/* Reference global state read by the solve path (8_band.h:77-110,218-225).   */
+/* Weak definitions live in the library.                                      */
+/* ------------------------------------------------------------------------- */
+extern int N_shape, isotropic, softening, include_strain, include_piezo, include_CME, PACKED;
+extern int myid, nprocs;
+extern int64_t N_H, na_rows, na_cols, na_rowsz, na_colsz, np_rows, np_cols, my_prow, my_pcol,
+    block_size;
+extern struct characteristic_functions *characteristic_function_G;
+extern struct strain_tensor strain_G;
+extern struct convolution_char_strain *convolutions_char_strain;
+extern struct piezo_potential phi_piezo_G;
+extern struct timing component_run_times;
+
+/* --- Reference routines, GPU implementations ------------------------------ */
+/* Replaces code/source/8_band/hamiltonian_8_band.c:23.  Writes the lower
+ * triangle of the column-major N_H x N_H Hamiltonian into the caller's H
+ * (host memory, leading dimension na_rows = N_H); the strict upper triangle
+ * is not written.  Reads characteristic_function_G, strain_G,
+ * convolutions_char_strain, phi_piezo_G, include_strain, include_piezo. */
+void hamiltonian_8_band(int N_shape, struct vector F, struct wave_vectors basis,
+                        struct supercell_geometry *supercell, struct material_params *parameters,
+                        qd_complex128 *H);
+
+/* Replaces code/source/8_band/diagonalise_hamiltonian.c:24 (zheevr with
+ * RANGE='I', UPLO='L').  idx_eig holds the 1-based window [il, iu]; eigval
+ * receives the iu-il+1 eigenvalues in ascending order, eigvec the
+ * eigenvectors (N_H x (iu-il+1), column-major).  H (lower triangle) is read. */
+void diagonalise_hamiltonian(int *idx_eig, qd_complex128 *H, double *eigval, qd_complex128 *eigvec);
+
+/* Replaces code/source/8_band/eigenstates.c:23.  Assembles H on the GPU from
+ * the global coefficient tables, solves the index window
+ * [6 N_PW - 2 N_vb, 6 N_PW + 2 N_cb - 1] and fills eigenstate_vb[0..2N_vb-1]
+ * and eigenstate_cb[0..2N_cb-1] (.E and .fourier, which the caller allocates
+ * with na_rows elements).  H never leaves the device. */
+void eigenstates(int N_shape, int *N_states, struct vector F, struct wave_vectors basis,
+                 struct supercell_geometry *supercell, struct material_params *parameters,
+                 struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb);
+
+/* Replaces code/source/8_band/coulomb_matrix_elements.c:24 for include_CME = 1
+ * (no multipole corrections) and a Coulomb cell equal to the electronic
+ * structure cell.  CME arrays are allocated by the caller with the sizes of
+ * 8_band_main.c:1752-1775. */
+void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coulomb_basis,
+                             struct supercell_geometry *supercell,
+                             struct material_params *parameters, int *N_states,
+                             struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb,
+                             struct coulomb_matrix_element CME, int coulomb_region_type);
+#endif /* QD_NO_REFERENCE_TYPES */
+
+/* ------------------------------------------------------------------------- */
+/* Status-returning API                                                       */
+/* ------------------------------------------------------------------------- */
+enum {
+    QD_OK = 0,
+    QD_ERR_INPUT = 1,        /* malformed or missing input file / key          */
+    QD_ERR_UNSUPPORTED = 2,  /* option outside the implemented path            */
+    QD_ERR_CUDA = 3,         /* CUDA runtime / device error                     */
+    QD_ERR_NOMEM = 4,        /* host or device allocation failed               */
+    QD_ERR_CONVERGENCE = 5,  /* eigensolver failed to converge                 */
+    QD_ERR_TIMEOUT = 6,      /* a bounded device-side wait ran out              */
+    QD_ERR_ARG = 7           /* invalid argument                               */
+};
+enum { QD_PREC_FP64 = 0, QD_PREC_MIXED = 1 };
+
+const char *qd_last_error_message(void);
+int qd_version(void);
+
+typedef struct qd_problem qd_problem;
+
+/* Parse parameters.in and supercell.in in `dir`; `overrides` are CLI-style
+ * "-Key=value" strings (read_command_line_input.c).  Computes the basis sets
+ * and material parameters on the host. */
+int qd_problem_load(const char *dir, const char *const *overrides, int n_overrides, qd_problem **out);
+void qd_problem_free(qd_problem *pr);
+/* Sizes: n_pw = N_Gx N_Gy N_Gz, n_h = 8 n_pw, window [lo, hi] 0-based. */
+int qd_problem_sizes(const qd_problem *pr, int64_t *n_pw, int64_t *n_h, int *lo, int *hi,
+                     int *n_vb, int *n_cb);
+/* Copies of the host-side set-up for checking: per-shape material parameters
+ * (n_shape structs) and geometry. */
+int qd_problem_materials(const qd_problem *pr, struct material_params *out, int n_shape);
+int qd_problem_geometry(const qd_problem *pr, struct supercell_geometry *out, int n_shape);
+
+/* Build every coefficient table on the GPU (shape transforms, strain, piezo
+ * potential, downsampling, convolutions, fused per-difference coefficients). */
+int qd_problem_build_tables(qd_problem *pr);
+/* Copy a table to host memory.  which: 0 chi (shape s), 1 strain component s
+ * (0..5 = xx yy zz yz xz xy), 2 piezo potential, 3 convolution (shape s,
+ * component c = 0..7 with 6 hydrostatic, 7 biaxial), 4 strain-cell chi,
+ * 5 strain-cell strain component s, 6 strain-cell piezo potential.
+ * out holds n_T elements (the grid of that cell). */
+int qd_problem_get_table(const qd_problem *pr, int which, int s, int c, qd_complex128 *out, int64_t n);
+
+/* Assemble H on the device.  mode 0: lower triangle only (the reference's
+ * layout), mode 1: full Hermitian.  H_dev is column-major N_H x N_H with leading
+ * dimension ld (>= N_H); complex128 (prec FP64) or complex64 (prec MIXED). */
+int qd_problem_assemble_dev(qd_problem *pr, void *H_dev, int64_t ld, int mode, int prec, void *stream);
+
+/* Eigenpairs of the problem's index window, H on the device (lower triangle,
+ * complex128, destroyed).  eigval_dev (M doubles) / eigvec_dev (N_H x M
+ * complex128) are device pointers.  prec QD_PREC_MIXED reduces a complex64
+ * copy on the tensor cores and refines in FP64 against H. */
+int qd_eigh_window_dev(int64_t n, void *H_dev, int64_t ld, int lo, int hi, int prec,
+                       double *eigval_dev, void *eigvec_dev, int64_t ldz, void *stream);
+
+/* Full solve for a loaded problem with host outputs: tables, assembly,
+ * eigensolve; eigval (M) and eigvec (N_H x M) in host memory. */
+int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *eigvec);
+
+/* Coulomb matrix elements (include_CME = 1 physics) for M_c states
+ * (eigvec_host: N_H x M_c, first 2 N_vb VB states then 2 N_cb CB states) into
+ * the reference's four output arrays (sizes of 8_band_main.c:1752-1755). */
+int qd_coulomb(qd_problem *pr, int n_vb_states, int n_cb_states, const qd_complex128 *eigvec_host,
+               qd_complex128 *hh, qd_complex128 *ee, qd_complex128 *eh_direct,
+               qd_complex128 *eh_exchange);
+
+/* Device plumbing for callers without their own CUDA binding.  qd_memcpy kind:
+ * 1 host->device, 2 device->host, 3 device->device.  Events time work on a
+ * stream (NULL = default stream). */
+int qd_dev_alloc(size_t bytes, void **out);
+int qd_dev_free(void *p);
+int qd_memcpy(void *dst, const void *src, size_t bytes, int kind);
+int qd_memset(void *dst, int value, size_t bytes);
+int qd_host_alloc_pinned(size_t bytes, void **out);
+int qd_host_free_pinned(void *p);
+int qd_device_synchronize(void);
+int qd_device_count(int *n);
+int qd_set_device(int dev);
+int qd_event_create(void **ev);
+int qd_event_record(void *ev, void *stream);
+int qd_event_elapsed_ms(void *ev0, void *ev1, float *ms);
+int qd_event_destroy(void *ev);
+
+/* Stage timings of the last qd_problem_solve / qd_eigh_window_dev call (ms):
+ * [0] assembly, [1] band reduction, [2] bulge chasing, [3] bisection,
+ * [4] inverse iteration, [5] back-transform, [6] refinement. */
+int qd_last_timings(double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUDOS_B200_H */

@@ -1,0 +1,223 @@
+// 8-band supercell Hamiltonian assembly (hamiltonian_8_band.c:23-500 with the
+// band functions of hamiltonian_8_band_matrix_elements.c:27-969).
+//
+// Every element H[(b1,G1),(b2,G2)] is a band-dependent polynomial in G1 and G2
+// whose coefficients depend only on the difference G1 - G2.  Those coefficients
+// are precomputed once per difference (fused_coef_kernel, 28 complex fields,
+// field-major so a warp's gathers are contiguous); this kernel then only
+// evaluates the polynomial and streams the result out.  It is bound by the
+// HBM write of H: 16 bytes per element (complex128), 8 (complex64), 24 (both).
+//
+// Layout: column-major, H[row + ld * col], row = band * N_PW + (ix N_y + iy) N_z + iz.
+// mode 0 writes the lower triangle only (the reference's layout; the strict upper
+// triangle of the caller's buffer is not touched); mode 1 writes both triangles
+// (upper = conjugate transpose, evaluated directly so every store stays coalesced).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "qd_complex.cuh"
+#include "qd_internal.h"
+
+namespace {
+
+enum { F_ZERO = 0, F_ECB, F_EHH, F_ELH, F_ESO, F_Q, F_R, F_RC, F_S, F_SC, F_TP, F_TM, F_U };
+
+// (row band, column band) for row band >= column band, 0-based (hamiltonian_8_band.c:78-492)
+__constant__ signed char c_func[8][8];
+__constant__ double c_fac[8][8];
+
+struct Ctx {
+    const double2 *__restrict__ coef;
+    int64_t nT;
+    const double *__restrict__ G[3];
+    int N[3], NT[3], off[3];
+    double K[3];
+};
+
+__device__ __forceinline__ zc ld(const Ctx &c, int k, int64_t t) { return zc(__ldg(&c.coef[k * c.nT + t])); }
+
+__device__ zc band_element(const Ctx &c, int rb, int cb, const int r[3], const int q[3]) {
+    int f = c_func[rb][cb];
+    if (f == F_ZERO) return zc(0.0);
+    int64_t t = ((int64_t)(r[0] - q[0] + c.NT[0] / 2) * c.NT[1] + (r[1] - q[1] + c.NT[1] / 2)) * c.NT[2] +
+                (r[2] - q[2] + c.NT[2] / 2);
+    double g1x = c.G[0][c.off[0] + r[0]], g1y = c.G[1][c.off[1] + r[1]], g1z = c.G[2][c.off[2] + r[2]];
+    double g2x = c.G[0][c.off[0] + q[0]], g2y = c.G[1][c.off[1] + q[1]], g2z = c.G[2][c.off[2] + q[2]];
+    double Kx = c.K[0], Ky = c.K[1], Kz = c.K[2];
+    double kinx = g1x * g2x + Kx * (g1x + g2x), kiny = g1y * g2y + Ky * (g1y + g2y),
+           kinz = g1z * g2z + Kz * (g1z + g2z);
+    const double H2 = 0.5 * QD_HBSQM;
+    zc v;
+    switch (f) {
+        case F_ECB:
+            v = ld(c, 0, t) + H2 * ld(c, 1, t) * (kinx + kiny + kinz + Kx * Kx + Ky * Ky + Kz * Kz) + ld(c, 13, t);
+            break;
+        case F_EHH:
+            v = ld(c, 2, t) - H2 * ld(c, 3, t) * (kinx + kiny + Kx * Kx + Ky * Ky) -
+                H2 * ld(c, 4, t) * (kinz + Kz * Kz) + ld(c, 14, t);
+            break;
+        case F_ELH:
+            v = ld(c, 5, t) - H2 * ld(c, 6, t) * (kinx + kiny + Kx * Kx + Ky * Ky) -
+                H2 * ld(c, 7, t) * (kinz + Kz * Kz) + ld(c, 15, t);
+            break;
+        case F_ESO:
+            v = ld(c, 8, t) - H2 * ld(c, 9, t) * (kinx + kiny + kinz + Kx * Kx + Ky * Ky + Kz * Kz) + ld(c, 16, t);
+            break;
+        case F_Q: {
+            zc g2 = ld(c, 10, t);
+            v = (-sqrt(0.5) * QD_HBSQM) * g2 * (kinx + kiny + Kx * Kx + Ky * Ky) +
+                (sqrt(2.0) * QD_HBSQM) * g2 * (kinz + Kz * Kz) + ld(c, 17, t);
+            break;
+        }
+        case F_R:
+        case F_RC: {
+            double sg = f == F_R ? -1.0 : 1.0;
+            double a = 0.5 * sqrt(3.0) * QD_HBSQM;
+            zc kin = a * ld(c, 10, t) * (kinx - kiny + Kx * Kx - Ky * Ky);
+            zc off = (sg * a) * ld(c, 11, t) * ((g1x + Kx) * (g2y + Ky) + (g1y + Ky) * (g2x + Kx));
+            zc rd = ld(c, 19, t);
+            v = kin + I_times(off) + ld(c, 18, t) - sg * I_times(rd);
+            break;
+        }
+        case F_S:
+        case F_SC: {
+            double sg = f == F_S ? -1.0 : 1.0;
+            double a = 0.5 * sqrt(1.5) * QD_HBSQM;
+            zc g3 = ld(c, 11, t);
+            zc re = a * g3 * ((g1x + Kx) * (g2z + Kz) + (g1z + Kz) * (g2x + Kx));
+            zc im = (sg * a) * g3 * ((g1y + Ky) * (g2z + Kz) + (g1z + Kz) * (g2y + Ky));
+            zc sxz = ld(c, 20, t), syz = ld(c, 21, t);
+            v = re + I_times(im) - sqrt(0.5) * (sxz + sg * I_times(syz));
+            break;
+        }
+        case F_TP:
+        case F_TM: {
+            double sg = f == F_TP ? 1.0 : -1.0;
+            double kx = g1x + g2x + 2 * Kx, ky = g1y + g2y + 2 * Ky, kz = g1z + g2z + 2 * Kz;
+            zc P = ld(c, 12, t);
+            zc Txx = ld(c, 22, t), Txy = ld(c, 23, t), Tyy = ld(c, 24, t), Txz = ld(c, 25, t), Tyz = ld(c, 26, t);
+            double c6 = -0.5 / sqrt(6.0);
+            zc s = (Txx + sg * I_times(Txy)) * kx + (Txy + sg * I_times(Tyy)) * ky + (Txz + sg * I_times(Tyz)) * kz;
+            v = (P * kx) / (2.0 * sqrt(6.0)) + sg * I_times(P * ky) / (2.0 * sqrt(6.0)) + c6 * s;
+            break;
+        }
+        case F_U: {
+            double kx = g1x + g2x + 2 * Kx, ky = g1y + g2y + 2 * Ky, kz = g1z + g2z + 2 * Kz;
+            zc P = ld(c, 12, t);
+            double c3 = -0.5 / sqrt(3.0);
+            v = (P * kz) / (2.0 * sqrt(3.0)) + c3 * (ld(c, 25, t) * kx + ld(c, 26, t) * ky + ld(c, 27, t) * kz);
+            break;
+        }
+    }
+    return c_fac[rb][cb] * v;
+}
+
+template <int OUT>  // OUT: 1 complex128, 2 complex64, 3 both
+__global__ void __launch_bounds__(128) assemble_kernel(Ctx c, int64_t npw, int64_t nh, double2 *__restrict__ H64,
+                                                       float2 *__restrict__ H32, int64_t ld, int full, int cols_per) {
+    int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t col0 = (int64_t)blockIdx.y * cols_per;
+    int64_t row_first = blockIdx.x * (int64_t)blockDim.x;
+    if (!full && row_first + blockDim.x - 1 < col0) return;  // tile entirely above the diagonal
+    if (row >= nh) return;
+    int rb = (int)(row / npw);
+    int i = (int)(row - rb * npw);
+    int r[3] = {i / (c.N[1] * c.N[2]), (i / c.N[2]) % c.N[1], i % c.N[2]};
+    int64_t col_end = col0 + cols_per < nh ? col0 + cols_per : nh;
+    for (int64_t col = col0; col < col_end; col++) {
+        if (!full && row < col) break;
+        int cb = (int)(col / npw);
+        int j = (int)(col - cb * npw);
+        int q[3] = {j / (c.N[1] * c.N[2]), (j / c.N[2]) % c.N[1], j % c.N[2]};
+        zc v;
+        if (row >= col) v = band_element(c, rb, cb, r, q);
+        else v = conj(band_element(c, cb, rb, q, r));
+        int64_t o = row + ld * col;
+        if (OUT & 1) __stcs(&H64[o], v.d2());
+        if (OUT & 2) __stcs(&H32[o], make_float2((float)v.re, (float)v.im));
+    }
+}
+
+int upload_block_map() {
+    static int done = 0;
+    if (done) return QD_OK;
+    signed char fn[8][8] = {{0}};
+    double fac[8][8] = {{0}};
+    const double s2 = sqrt(2.0), s3 = sqrt(3.0);
+    struct E { int r, c, f; double a; } m[] = {
+        {1, 1, F_ECB, 1}, {2, 1, F_TM, -s3}, {3, 1, F_U, s2}, {4, 1, F_U, -1}, {7, 1, F_TP, -1}, {8, 1, F_TP, -s2},
+        {2, 2, F_EHH, 1}, {3, 2, F_SC, s2}, {4, 2, F_SC, -1}, {7, 2, F_RC, -1}, {8, 2, F_RC, -s2},
+        {3, 3, F_ELH, 1}, {4, 3, F_Q, 1}, {5, 3, F_TP, 1}, {6, 3, F_RC, 1}, {8, 3, F_SC, s3},
+        {4, 4, F_ESO, 1}, {5, 4, F_TP, s2}, {6, 4, F_RC, s2}, {7, 4, F_SC, -s3},
+        {5, 5, F_ECB, 1}, {6, 5, F_TP, -s3}, {7, 5, F_U, s2}, {8, 5, F_U, -1},
+        {6, 6, F_EHH, 1}, {7, 6, F_S, s2}, {8, 6, F_S, -1},
+        {7, 7, F_ELH, 1}, {8, 7, F_Q, 1},
+        {8, 8, F_ESO, 1}};
+    for (auto &e : m) {
+        fn[e.r - 1][e.c - 1] = (signed char)e.f;
+        fac[e.r - 1][e.c - 1] = e.a;
+    }
+    if (cudaMemcpyToSymbol(c_func, fn, sizeof(fn)) != cudaSuccess) return QD_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_fac, fac, sizeof(fac)) != cudaSuccess) return QD_ERR_CUDA;
+    done = 1;
+    return QD_OK;
+}
+
+}  // namespace
+
+extern "C" int qd_assemble_launch(const void *d_coef, const double *d_Gx, const double *d_Gy, const double *d_Gz,
+                                  const int N[3], const double K[3], void *H, int64_t ld, int mode, int prec,
+                                  void *stream) {
+    if (upload_block_map() != QD_OK) return qd_set_error(QD_ERR_CUDA, "block map upload failed");
+    Ctx c;
+    c.coef = (const double2 *)d_coef;
+    c.G[0] = d_Gx; c.G[1] = d_Gy; c.G[2] = d_Gz;
+    for (int a = 0; a < 3; a++) {
+        c.N[a] = N[a];
+        c.NT[a] = 2 * N[a] - 1;
+        c.off[a] = c.NT[a] / 2 - N[a] / 2;
+        c.K[a] = K[a];
+    }
+    c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
+    int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
+    if (ld < nh) return qd_set_error(QD_ERR_ARG, "leading dimension %lld < N_H %lld", (long long)ld, (long long)nh);
+    const int cols_per = 16;
+    dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
+    cudaStream_t st = (cudaStream_t)stream;
+    int full = mode == 1;
+    if (prec == QD_PREC_FP64)
+        assemble_kernel<1><<<grid, 128, 0, st>>>(c, npw, nh, (double2 *)H, nullptr, ld, full, cols_per);
+    else if (prec == QD_PREC_MIXED)
+        assemble_kernel<2><<<grid, 128, 0, st>>>(c, npw, nh, nullptr, (float2 *)H, ld, full, cols_per);
+    else
+        return qd_set_error(QD_ERR_ARG, "unknown precision %d", prec);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
+// Both copies in one pass: complex128 into H64 and complex64 into H32 (same ld).
+extern "C" int qd_assemble_dual_launch(const void *d_coef, const double *d_Gx, const double *d_Gy,
+                                       const double *d_Gz, const int N[3], const double K[3], void *H64,
+                                       void *H32, int64_t ld, int mode, void *stream) {
+    if (upload_block_map() != QD_OK) return qd_set_error(QD_ERR_CUDA, "block map upload failed");
+    Ctx c;
+    c.coef = (const double2 *)d_coef;
+    c.G[0] = d_Gx; c.G[1] = d_Gy; c.G[2] = d_Gz;
+    for (int a = 0; a < 3; a++) {
+        c.N[a] = N[a];
+        c.NT[a] = 2 * N[a] - 1;
+        c.off[a] = c.NT[a] / 2 - N[a] / 2;
+        c.K[a] = K[a];
+    }
+    c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
+    int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
+    const int cols_per = 16;
+    dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
+    assemble_kernel<3><<<grid, 128, 0, (cudaStream_t)stream>>>(c, npw, nh, (double2 *)H64, (float2 *)H32, ld,
+                                                                mode == 1, cols_per);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
+    return QD_OK;
+}

@@ -1,0 +1,92 @@
+// Shared pieces of the eigensolver kernels: complex scalar templates, block
+// reductions and a bounded grid barrier for cooperative launches.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+template <typename R>
+struct cpx {
+    R re, im;
+};
+
+template <typename R>
+__device__ __forceinline__ cpx<R> mk(R a, R b) {
+    cpx<R> z;
+    z.re = a;
+    z.im = b;
+    return z;
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> cadd(cpx<R> a, cpx<R> b) { return mk<R>(a.re + b.re, a.im + b.im); }
+template <typename R>
+__device__ __forceinline__ cpx<R> csub(cpx<R> a, cpx<R> b) { return mk<R>(a.re - b.re, a.im - b.im); }
+template <typename R>
+__device__ __forceinline__ cpx<R> cmul(cpx<R> a, cpx<R> b) {
+    return mk<R>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+// conj(a) * b
+template <typename R>
+__device__ __forceinline__ cpx<R> cmulc(cpx<R> a, cpx<R> b) {
+    return mk<R>(a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re);
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> cconj(cpx<R> a) { return mk<R>(a.re, -a.im); }
+template <typename R>
+__device__ __forceinline__ R cabs2(cpx<R> a) { return a.re * a.re + a.im * a.im; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over the block of one double; every thread gets the result.  `scratch`
+// holds >= 33 doubles in shared memory.
+__device__ __forceinline__ double block_sum(double v, double *scratch) {
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double t = lane < nw ? scratch[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) scratch[32] = t;
+    }
+    __syncthreads();
+    return scratch[32];
+}
+
+// Grid barrier for kernels launched cooperatively (all blocks co-resident).
+// bar[0] counts arrivals, bar[1] is the generation.  The wait is bounded: after
+// `limit` polls the block records QD_ERR_TIMEOUT-style failure in *err and the
+// barrier returns false, so a kernel whose peer has died exits instead of
+// hanging.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err, long long limit) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned *gen = bar + 1;
+        unsigned g = *gen;
+        __threadfence();
+        unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (++it > limit || *(volatile int *)err) {
+                    atomicExch(err, 6);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}

@@ -1,0 +1,476 @@
+// Partial Hermitian eigensolver for an index window [lo, hi] (the zheevr
+// RANGE='I' call of diagonalise_hamiltonian.c:55-77), on one GPU.
+//
+// FP64 path:  stage 1 (dense -> band, FP64) -> stage 2 (band -> tridiagonal)
+//             -> bisection for [lo, hi] -> band inverse iteration -> Q1 back-transform.
+// Mixed path: stage 1 on a complex64 copy (tensor-core CGEMMs) -> stage 2,
+//             bisection and inverse iteration in FP64 on that band for
+//             [lo - g, hi + g] (g guard states on each side) -> complex64
+//             back-transform -> one FP64 Rayleigh-Ritz step against the FP64 H
+//             (Y = H X with ZHEMM, k x k generalized Hermitian eigenproblem by
+//             Cholesky + Jacobi in one block) -> the window's eigenpairs.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "eig_common.cuh"
+#include "qd_internal.h"
+
+typedef cpx<double> zd;
+
+struct Stage1Work {
+    void *VT, *X, *M, *Y, *Tall, *Rall;
+    double *red;
+    unsigned *bar;
+    int *err;
+    int npanels;
+};
+extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w);
+extern "C" void qd_stage1_free(Stage1Work *w);
+extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, Stage1Work *w, void *stream);
+extern "C" int qd_extract_band(const void *A, int64_t n, int64_t lda, int b, int fp32, const Stage1Work *w,
+                               double2 *AB, int ldb, void *stream);
+extern "C" int qd_stage1_backtransform(const void *A, int64_t n, int64_t lda, int b, int fp32, const Stage1Work *w,
+                                       void *Z, int64_t ldz, int mz, void *stream);
+extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *err, void *stream);
+extern "C" int qd_tridiag_bisect(const double2 *AB, int ldb, int n, int lo, int hi, double *d, double *e2,
+                                 double *bounds, double *w, void *stream);
+extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const double *lam_dev, int ngroups,
+                             const int *gstart_dev, const int *gsize_dev, double2 *Lw, double2 *Uw, int *ipivw,
+                             double2 *Z, int64_t ldz, double bnorm, double2 *ywork, void *stream);
+extern "C" cublasHandle_t qd_cublas(void);
+
+static double g_timings[8];
+extern "C" int qd_last_timings(double *ms, int n) {
+    for (int i = 0; i < n && i < 8; i++) ms[i] = g_timings[i];
+    return QD_OK;
+}
+extern "C" void qd_set_timing(int i, double ms) {
+    if (i >= 0 && i < 8) g_timings[i] = ms;
+}
+
+#define CUDA_OK(x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess)                                                                        \
+            return qd_set_error(QD_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    } while (0)
+#define BLAS_OK(x)                                                                                   \
+    do {                                                                                             \
+        cublasStatus_t s_ = (x);                                                                     \
+        if (s_ != CUBLAS_STATUS_SUCCESS)                                                             \
+            return qd_set_error(QD_ERR_CUDA, "%s:%d cuBLAS status %d", __FILE__, __LINE__, (int)s_); \
+    } while (0)
+#define RC(x)                         \
+    do {                              \
+        int rc_ = (x);                \
+        if (rc_ != QD_OK) return rc_; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------
+// full Hermitian complex64 copy of a complex128 lower triangle
+__global__ void lower64_to_full32_kernel(const double2 *H, int64_t ld, int64_t n, float2 *H32, int64_t ld32) {
+    int64_t col = blockIdx.y;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = row >= col ? H[row + col * ld] : H[col + row * ld];
+        if (row < col) v.y = -v.y;
+        if (row == col) v.y = 0.0;
+        H32[row + col * ld32] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+__global__ void c128_to_c64_kernel(const double2 *a, int64_t lda, float2 *b, int64_t ldb, int64_t n) {
+    int64_t col = blockIdx.y;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = a[i + col * lda];
+        b[i + col * ldb] = make_float2((float)v.x, (float)v.y);
+    }
+}
+__global__ void c64_to_c128_kernel(const float2 *a, int64_t lda, double2 *b, int64_t ldb, int64_t n) {
+    int64_t col = blockIdx.y;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float2 v = a[i + col * lda];
+        b[i + col * ldb] = make_double2((double)v.x, (double)v.y);
+    }
+}
+
+// Max |B_ij| of the band (a norm estimate for the inverse-iteration pivot floor).
+__global__ void band_absmax_kernel(const double2 *AB, int ldb, int64_t n, int b, unsigned long long *out) {
+    double m = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+        for (int d = 0; d <= b; d++) {
+            double2 v = AB[d + j * ldb];
+            m = fmax(m, sqrt(v.x * v.x + v.y * v.y));
+        }
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));  // non-negative doubles order as integers
+}
+
+// Rayleigh-Ritz on k vectors: S = X^H X, A = X^H (H X) (k x k, column-major,
+// global).  Solves A c = theta S c: S = L L^H, A' = L^-1 A L^-H, Jacobi on A',
+// C = L^-H C'.  theta ascending.  One block.
+__global__ void __launch_bounds__(256) small_rr_kernel(int k, double2 *S, double2 *A, double2 *C, double *theta,
+                                                       int *info) {
+    __shared__ double scratch[33];
+    // Cholesky S = L L^H (lower, in place)
+    for (int j = 0; j < k; j++) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double d = S[j + j * k].x;
+            for (int p = 0; p < j; p++) d -= S[j + p * k].x * S[j + p * k].x + S[j + p * k].y * S[j + p * k].y;
+            if (!(d > 0.0)) { *info = 1; d = 1e-300; }
+            S[j + j * k] = make_double2(sqrt(d), 0.0);
+        }
+        __syncthreads();
+        double ljj = S[j + j * k].x;
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) {
+            double2 s = S[i + j * k];
+            for (int p = 0; p < j; p++) {  // s -= L[i,p] conj(L[j,p])
+                double2 a = S[i + p * k], b = S[j + p * k];
+                s.x -= a.x * b.x + a.y * b.y;
+                s.y -= a.y * b.x - a.x * b.y;
+            }
+            S[i + j * k] = make_double2(s.x / ljj, s.y / ljj);
+        }
+    }
+    __syncthreads();
+    // A <- L^-1 A (forward substitution on each column), then A <- A L^-H (on rows)
+    for (int c = threadIdx.x; c < k; c += blockDim.x) {
+        for (int i = 0; i < k; i++) {
+            double2 s = A[i + c * k];
+            for (int p = 0; p < i; p++) {
+                double2 l = S[i + p * k], a = A[p + c * k];
+                s.x -= l.x * a.x - l.y * a.y;
+                s.y -= l.x * a.y + l.y * a.x;
+            }
+            double d = S[i + i * k].x;
+            A[i + c * k] = make_double2(s.x / d, s.y / d);
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < k; r += blockDim.x) {
+        // row r: x L^H = a  ->  x_i = (a_i - sum_{p<i} x_p conj(L[i,p])) / L[i,i]
+        for (int i = 0; i < k; i++) {
+            double2 s = A[r + i * k];
+            for (int p = 0; p < i; p++) {
+                double2 x = A[r + p * k], l = S[i + p * k];
+                s.x -= x.x * l.x + x.y * l.y;
+                s.y -= x.y * l.x - x.x * l.y;
+            }
+            double d = S[i + i * k].x;
+            A[r + i * k] = make_double2(s.x / d, s.y / d);
+        }
+    }
+    __syncthreads();
+    // symmetrize, C' = I
+    for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
+        int i = idx % k, j = idx / k;
+        if (i > j) {
+            double2 a = A[i + j * k], b = A[j + i * k];
+            double2 m = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+            A[i + j * k] = m;
+            A[j + i * k] = make_double2(m.x, -m.y);
+        } else if (i == j) {
+            A[i + i * k].y = 0.0;
+        }
+        C[idx] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    // cyclic Jacobi with round-robin pairing (k padded to even)
+    int kk = k + (k & 1);
+    __shared__ int pp[128], qq[128];
+    __shared__ double jc[64], js[64], jpr[64], jpi[64];  // rotation per pair: c, s, e^{-i phi}
+    for (int sweep = 0; sweep < 30; sweep++) {
+        double off = 0.0;
+        for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
+            int i = idx % k, j = idx / k;
+            if (i != j) off += A[idx].x * A[idx].x + A[idx].y * A[idx].y;
+        }
+        off = block_sum(off, scratch);
+        double dn = 0.0;
+        for (int i = threadIdx.x; i < k; i += blockDim.x) dn += A[i + i * k].x * A[i + i * k].x;
+        dn = block_sum(dn, scratch);
+        if (off <= 1e-30 * dn || off == 0.0) break;
+        for (int round = 0; round < kk - 1; round++) {
+            // pairs: position 0 fixed, others rotate
+            for (int t = threadIdx.x; t < kk / 2; t += blockDim.x) {
+                int a = t == 0 ? 0 : 1 + (t - 1 + round) % (kk - 1);
+                int bpos = kk - 1 - t;
+                int b = 1 + (bpos - 1 + round) % (kk - 1);
+                int p = a < b ? a : b, q = a < b ? b : a;
+                pp[t] = p;
+                qq[t] = q;
+                double c = 1.0, s = 0.0, er = 1.0, ei = 0.0;
+                if (q < k) {
+                    double app = A[p + p * k].x, aqq = A[q + q * k].x;
+                    double2 apq = A[p + q * k];
+                    double mag = sqrt(apq.x * apq.x + apq.y * apq.y);
+                    if (mag > 1e-300) {
+                        er = apq.x / mag;   // e^{-i phi} with phi = arg(apq): (cos phi, -sin phi)
+                        ei = -apq.y / mag;
+                        double th = (aqq - app) / (2.0 * mag);
+                        double t_ = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                        c = 1.0 / sqrt(t_ * t_ + 1.0);
+                        s = t_ * c;
+                    }
+                }
+                jc[t] = c; js[t] = s; jpr[t] = er; jpi[t] = ei;
+            }
+            __syncthreads();
+            // rows: A <- J^H A  with J = [[c, s], [-s e, c e]] on (p, q), e = e^{-i phi}
+            for (int idx = threadIdx.x; idx < (kk / 2) * k; idx += blockDim.x) {
+                int t = idx / k, col = idx % k;
+                int p = pp[t], q = qq[t];
+                if (q >= k) continue;
+                double c = jc[t], s = js[t], er = jpr[t], ei = jpi[t];
+                double2 ap = A[p + col * k], aq = A[q + col * k];
+                // conj(j21) = -s conj(e), conj(j22) = c conj(e); conj(e) = (er, -ei)
+                double2 eq = make_double2(er * aq.x + ei * aq.y, er * aq.y - ei * aq.x);  // conj(e) * aq
+                A[p + col * k] = make_double2(c * ap.x - s * eq.x, c * ap.y - s * eq.y);
+                A[q + col * k] = make_double2(s * ap.x + c * eq.x, s * ap.y + c * eq.y);
+            }
+            __syncthreads();
+            // columns: A <- A J, C <- C J
+            for (int idx = threadIdx.x; idx < (kk / 2) * k * 2; idx += blockDim.x) {
+                int which = idx / ((kk / 2) * k);
+                int r2 = idx % ((kk / 2) * k);
+                int t = r2 / k, row = r2 % k;
+                int p = pp[t], q = qq[t];
+                if (q >= k) continue;
+                double c = jc[t], s = js[t], er = jpr[t], ei = jpi[t];
+                double2 *M = which == 0 ? A : C;
+                double2 xp = M[row + p * k], xq = M[row + q * k];
+                // new_p = xp c + xq (-s e) ; new_q = xp s + xq (c e)
+                double2 xe = make_double2(xq.x * er - xq.y * ei, xq.x * ei + xq.y * er);  // xq * e
+                M[row + p * k] = make_double2(c * xp.x - s * xe.x, c * xp.y - s * xe.y);
+                M[row + q * k] = make_double2(s * xp.x + c * xe.x, s * xp.y + c * xe.y);
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    // sort ascending (selection sort on thread 0), permute C' columns
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < k; i++) theta[i] = A[i + i * k].x;
+        for (int i = 0; i < k; i++) {
+            int m = i;
+            for (int j = i + 1; j < k; j++)
+                if (theta[j] < theta[m]) m = j;
+            if (m != i) {
+                double t = theta[i]; theta[i] = theta[m]; theta[m] = t;
+                for (int r = 0; r < k; r++) {
+                    double2 x = C[r + i * k]; C[r + i * k] = C[r + m * k]; C[r + m * k] = x;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // C <- L^-H C'  (back substitution with L^H)
+    for (int c = threadIdx.x; c < k; c += blockDim.x) {
+        for (int i = k - 1; i >= 0; i--) {
+            double2 s = C[i + c * k];
+            for (int p = i + 1; p < k; p++) {  // (L^H)[i,p] = conj(L[p,i])
+                double2 l = S[p + i * k], x = C[p + c * k];
+                s.x -= l.x * x.x + l.y * x.y;
+                s.y -= l.x * x.y - l.y * x.x;
+            }
+            double d = S[i + i * k].x;
+            C[i + c * k] = make_double2(s.x / d, s.y / d);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+struct Timer {
+    cudaEvent_t e[10];
+    int n = 0;
+    cudaStream_t st;
+    explicit Timer(cudaStream_t s) : st(s) {
+        for (int i = 0; i < 10; i++) cudaEventCreate(&e[i]);
+    }
+    ~Timer() {
+        for (int i = 0; i < 10; i++) cudaEventDestroy(e[i]);
+    }
+    void mark() {
+        if (n < 10) cudaEventRecord(e[n++], st);
+    }
+    double ms(int a, int b) {
+        float t = 0;
+        cudaEventElapsedTime(&t, e[a], e[b]);
+        return t;
+    }
+};
+
+static int block_size_default() {
+    const char *s = getenv("QD_BAND");
+    int b = s ? atoi(s) : 32;
+    if (b < 8) b = 8;
+    if (b > 32) b = 32;
+    return b;
+}
+
+extern "C" int qd_mixed_guard(void) {
+    const char *s = getenv("QD_GUARD");
+    return s ? atoi(s) : 8;
+}
+
+extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, int prec, double *w_dev, void *Z_dev,
+                              int64_t ldz, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (lo < 0 || hi >= n || lo > hi) return qd_set_error(QD_ERR_ARG, "bad eigenvalue window [%d, %d] for n=%lld", lo, hi, (long long)n);
+    if (n > 0x7fffffff / 2) return qd_set_error(QD_ERR_UNSUPPORTED, "matrix too large");
+    int b = block_size_default();
+    if (b > n - 1) b = (int)(n > 2 ? n - 1 : 1);
+    const int mixed = prec == QD_PREC_MIXED;
+    int g = mixed ? qd_mixed_guard() : 0;
+    int lo2 = lo - g < 0 ? 0 : lo - g, hi2 = hi + g > n - 1 ? (int)n - 1 : hi + g;
+    int k = hi2 - lo2 + 1, M = hi - lo + 1;
+    int ldb = 2 * b + 1;
+    Timer tm(st);
+    tm.mark();  // 0
+    // ---- stage 1
+    void *A = H;
+    int64_t lda = ld;
+    float2 *H32 = nullptr;
+    if (mixed) {
+        CUDA_OK(cudaMalloc(&H32, sizeof(float2) * n * n));
+        lower64_to_full32_kernel<<<dim3((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)n), 256, 0, st>>>(
+            (const double2 *)H, ld, n, H32, n);
+        CUDA_OK(cudaGetLastError());
+        A = H32;
+        lda = n;
+    }
+    Stage1Work w1;
+    RC(qd_stage1_alloc(n, b, mixed ? 8 : 16, &w1));
+    RC(qd_stage1_run(A, n, lda, b, mixed, &w1, st));
+    tm.mark();  // 1
+    // ---- band, stage 2, bisection
+    double2 *AB, *AB0, *Zb;
+    double *d, *e2, *bounds, *lam;
+    int *progress, *err;
+    CUDA_OK(cudaMalloc(&AB, sizeof(double2) * n * ldb));
+    CUDA_OK(cudaMalloc(&AB0, sizeof(double2) * n * ldb));
+    CUDA_OK(cudaMalloc(&d, sizeof(double) * n));
+    CUDA_OK(cudaMalloc(&e2, sizeof(double) * n));
+    CUDA_OK(cudaMalloc(&bounds, sizeof(double) * 4));
+    CUDA_OK(cudaMalloc(&lam, sizeof(double) * k));
+    CUDA_OK(cudaMalloc(&progress, sizeof(int) * n));
+    CUDA_OK(cudaMalloc(&err, sizeof(int)));
+    RC(qd_extract_band(A, n, lda, b, mixed, &w1, AB, ldb, st));
+    CUDA_OK(cudaMemcpyAsync(AB0, AB, sizeof(double2) * n * ldb, cudaMemcpyDeviceToDevice, st));
+    RC(qd_hb2st(AB, ldb, (int)n, b, progress, err, st));
+    int herr = 0;
+    CUDA_OK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (herr) return qd_set_error(QD_ERR_TIMEOUT, "band reduction: wait on the previous sweep ran out");
+    tm.mark();  // 2
+    RC(qd_tridiag_bisect(AB, ldb, (int)n, lo2, hi2, d, e2, bounds, lam, st));
+    std::vector<double> lam_h(k);
+    CUDA_OK(cudaMemcpyAsync(lam_h.data(), lam, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+    unsigned long long *dmax;
+    CUDA_OK(cudaMalloc(&dmax, sizeof(unsigned long long)));
+    CUDA_OK(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st));
+    band_absmax_kernel<<<64, 256, 0, st>>>(AB0, ldb, n, b, dmax);
+    unsigned long long bm_bits = 0;
+    CUDA_OK(cudaMemcpyAsync(&bm_bits, dmax, sizeof(bm_bits), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    tm.mark();  // 3
+    double bnorm;
+    memcpy(&bnorm, &bm_bits, sizeof(double));
+    bnorm *= (double)(2 * b + 1);
+    // groups of numerically degenerate eigenvalues share one LU factorisation
+    std::vector<int> gs, gz;
+    double tol_deg = 1e-10 * (bnorm > 1.0 ? bnorm : 1.0);
+    for (int i = 0; i < k; i++) {
+        if (i > 0 && fabs(lam_h[i] - lam_h[i - 1]) <= tol_deg && gz.back() < 8) gz.back()++;
+        else { gs.push_back(i); gz.push_back(1); }
+    }
+    int ng = (int)gs.size();
+    int *gs_d, *gz_d, *ipiv;
+    double2 *Lw, *Uw, *yw;
+    CUDA_OK(cudaMalloc(&gs_d, sizeof(int) * ng));
+    CUDA_OK(cudaMalloc(&gz_d, sizeof(int) * ng));
+    CUDA_OK(cudaMemcpyAsync(gs_d, gs.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(gz_d, gz.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMalloc(&Lw, sizeof(double2) * (size_t)ng * n * b));
+    CUDA_OK(cudaMalloc(&Uw, sizeof(double2) * (size_t)ng * n * (2 * b + 1)));
+    CUDA_OK(cudaMalloc(&ipiv, sizeof(int) * (size_t)ng * n));
+    CUDA_OK(cudaMalloc(&yw, sizeof(double2) * (size_t)ng * 8 * n));
+    CUDA_OK(cudaMalloc(&Zb, sizeof(double2) * n * k));
+    RC(qd_band_invit(AB0, ldb, (int)n, b, lam, ng, gs_d, gz_d, Lw, Uw, ipiv, Zb, n, bnorm, yw, st));
+    tm.mark();  // 4
+    // ---- back-transform
+    if (!mixed) {
+        RC(qd_stage1_backtransform(A, n, lda, b, 0, &w1, Zb, n, k, st));
+        tm.mark();  // 5
+        CUDA_OK(cudaMemcpy2DAsync(Z_dev, sizeof(double2) * ldz, Zb, sizeof(double2) * n, sizeof(double2) * n, M,
+                                  cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(w_dev, lam, sizeof(double) * M, cudaMemcpyDeviceToDevice, st));
+        tm.mark();  // 6
+    } else {
+        float2 *Z32;
+        CUDA_OK(cudaMalloc(&Z32, sizeof(float2) * n * k));
+        c128_to_c64_kernel<<<dim3(64, k), 256, 0, st>>>(Zb, n, Z32, n, n);
+        RC(qd_stage1_backtransform(A, n, lda, b, 1, &w1, Z32, n, k, st));
+        c64_to_c128_kernel<<<dim3(64, k), 256, 0, st>>>(Z32, n, Zb, n, n);
+        CUDA_OK(cudaGetLastError());
+        tm.mark();  // 5
+        // ---- FP64 Rayleigh-Ritz against H (lower triangle, complex128)
+        cublasHandle_t h = qd_cublas();
+        BLAS_OK(cublasSetStream(h, st));
+        double2 *Y, *S, *Ak, *C, *Xn;
+        double *theta;
+        int *info;
+        CUDA_OK(cudaMalloc(&Y, sizeof(double2) * n * k));
+        CUDA_OK(cudaMalloc(&Xn, sizeof(double2) * n * k));
+        CUDA_OK(cudaMalloc(&S, sizeof(double2) * k * k));
+        CUDA_OK(cudaMalloc(&Ak, sizeof(double2) * k * k));
+        CUDA_OK(cudaMalloc(&C, sizeof(double2) * k * k));
+        CUDA_OK(cudaMalloc(&theta, sizeof(double) * k));
+        CUDA_OK(cudaMalloc(&info, sizeof(int)));
+        CUDA_OK(cudaMemsetAsync(info, 0, sizeof(int), st));
+        const cuDoubleComplex one = {1, 0}, zero = {0, 0};
+        BLAS_OK(cublasZhemm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, (int)n, k, &one, (cuDoubleComplex *)H, (int)ld,
+                            (cuDoubleComplex *)Zb, (int)n, &zero, (cuDoubleComplex *)Y, (int)n));
+        BLAS_OK(cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, k, k, (int)n, &one, (cuDoubleComplex *)Zb, (int)n,
+                            (cuDoubleComplex *)Zb, (int)n, &zero, (cuDoubleComplex *)S, k));
+        BLAS_OK(cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, k, k, (int)n, &one, (cuDoubleComplex *)Zb, (int)n,
+                            (cuDoubleComplex *)Y, (int)n, &zero, (cuDoubleComplex *)Ak, k));
+        small_rr_kernel<<<1, 256, 0, st>>>(k, S, Ak, C, theta, info);
+        CUDA_OK(cudaGetLastError());
+        BLAS_OK(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, k, k, &one, (cuDoubleComplex *)Zb, (int)n,
+                            (cuDoubleComplex *)C, k, &zero, (cuDoubleComplex *)Xn, (int)n));
+        int off = lo - lo2;
+        CUDA_OK(cudaMemcpy2DAsync(Z_dev, sizeof(double2) * ldz, Xn + (int64_t)off * n, sizeof(double2) * n,
+                                  sizeof(double2) * n, M, cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(w_dev, theta + off, sizeof(double) * M, cudaMemcpyDeviceToDevice, st));
+        int hinfo = 0;
+        CUDA_OK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        tm.mark();  // 6
+        CUDA_OK(cudaStreamSynchronize(st));
+        cudaFree(Y); cudaFree(Xn); cudaFree(S); cudaFree(Ak); cudaFree(C); cudaFree(theta); cudaFree(info);
+        cudaFree(Z32);
+        if (hinfo) return qd_set_error(QD_ERR_CONVERGENCE, "Rayleigh-Ritz: Gram matrix not positive definite");
+    }
+    CUDA_OK(cudaStreamSynchronize(st));
+    g_timings[1] = tm.ms(0, 1);
+    g_timings[2] = tm.ms(1, 2);
+    g_timings[3] = tm.ms(2, 3);
+    g_timings[4] = tm.ms(3, 4);
+    g_timings[5] = tm.ms(4, 5);
+    g_timings[6] = tm.ms(5, 6);
+    cudaFree(AB); cudaFree(AB0); cudaFree(d); cudaFree(e2); cudaFree(bounds); cudaFree(lam); cudaFree(progress);
+    cudaFree(err); cudaFree(dmax); cudaFree(gs_d); cudaFree(gz_d); cudaFree(Lw); cudaFree(Uw); cudaFree(ipiv);
+    cudaFree(yw); cudaFree(Zb);
+    if (H32) cudaFree(H32);
+    qd_stage1_free(&w1);
+    return QD_OK;
+}

@@ -1,0 +1,577 @@
+// Stage 2 of the eigensolver and the tridiagonal / band eigenvector steps.
+//
+//  * hb2st_kernel: Hermitian band (half bandwidth b) -> real-diagonal
+//    tridiagonal by Householder bulge chasing, eigenvalues only.  Sweep s
+//    annihilates column s below the subdiagonal and chases the bulge down the
+//    band in tasks of b rows.  Sweeps run concurrently in a persistent
+//    cooperative kernel, one sweep per block at a time: task k of sweep s touches
+//    rows/columns [s+1+(k-1)b, s+(k+1)b] and may start once sweep s-1 has
+//    finished its tasks 0..k+2 (the last one overlapping that range).  The wait
+//    on the predecessor's progress counter is bounded.
+//  * bisect_kernel: eigenvalues of the tridiagonal matrix with indices [lo, hi]
+//    by multisection on Sturm counts (one warp per eigenvalue, 32 shifts per
+//    step).  Selecting by index reproduces zheevr's RANGE='I' window.
+//  * band_invit_kernel: eigenvectors of the band matrix by inverse iteration:
+//    LU with partial pivoting of (B - lambda I) in a shared-memory window that
+//    slides down the band, then three solves with the starting block of the
+//    whole group of (numerically) degenerate eigenvalues and Gram-Schmidt within
+//    the group (Kramers pairs are exactly degenerate).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+
+#include "eig_common.cuh"
+#include "qd_internal.h"
+
+typedef cpx<double> zd;
+
+#define SPIN_LIMIT (1LL << 25)
+#define PROGRESS_DONE 0x7fffffff
+
+// ---------------------------------------------------------------------------
+// Householder helpers in shared memory (one warp computes, results broadcast)
+// ---------------------------------------------------------------------------
+// x[0..len) -> v (v[0] = 1), returns beta (real) and tau; zlarfg conventions.
+__device__ void larfg_warp(zd *x, int len, double *beta_out, zd *tau_out) {
+    int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int i = 1 + lane; i < len; i += 32) s += cabs2(x[i]);
+    s = warp_sum(s);
+    zd alpha = x[0];
+    double beta;
+    zd tau, scale;
+    if (s == 0.0 && alpha.im == 0.0) {
+        beta = alpha.re;
+        tau = mk<double>(0, 0);
+        scale = mk<double>(0, 0);
+    } else {
+        beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + s), alpha.re);
+        tau = mk<double>((beta - alpha.re) / beta, -alpha.im / beta);
+        double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
+        scale = mk<double>(dr / den, -di / den);
+    }
+    __syncwarp();
+    for (int i = 1 + lane; i < len; i += 32) x[i] = cmul(x[i], scale);
+    if (lane == 0) x[0] = mk<double>(1, 0);
+    __syncwarp();
+    *beta_out = beta;
+    *tau_out = tau;
+}
+
+// D (n x n full Hermitian, ld) <- H^H D H, H = I - tau v v^H.
+__device__ void sym_update(zd *D, int ld, int n, const zd *v, zd tau, zd *w, double *scratch) {
+    // w = tau D v
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        zd acc = mk<double>(0, 0);
+        for (int c = 0; c < n; c++) acc = cadd(acc, cmul(D[r + c * ld], v[c]));
+        w[r] = cmul(tau, acc);
+    }
+    __syncthreads();
+    // c = Re(conj(tau) v^H w) ... (real for Hermitian D)
+    double part = 0.0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        zd t = cmulc(v[r], w[r]);   // conj(v) w
+        zd ct = cmulc(tau, t);      // conj(tau) * t
+        part += ct.re;
+    }
+    double cc = block_sum(part, scratch);
+    for (int r = threadIdx.x; r < n; r += blockDim.x) w[r] = csub(w[r], mk<double>(0.5 * cc * v[r].re, 0.5 * cc * v[r].im));
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        int r = idx % n, c = idx / n;
+        // D -= v w^H + w v^H
+        zd a = cmul(v[r], cconj(w[c]));
+        zd b = cmul(w[r], cconj(v[c]));
+        D[r + c * ld] = csub(D[r + c * ld], cadd(a, b));
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ zd ldab(const double2 *AB, int ldb, int64_t i, int64_t j) {  // i >= j
+    double2 v = __ldcg(&AB[(i - j) + j * (int64_t)ldb]);
+    return mk<double>(v.x, v.y);
+}
+__device__ __forceinline__ void stab(double2 *AB, int ldb, int64_t i, int64_t j, zd v) {
+    __stcg(&AB[(i - j) + j * (int64_t)ldb], make_double2(v.re, v.im));
+}
+
+__device__ bool wait_progress(volatile int *progress, int s_prev, int need, int *err) {
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        long long it = 0;
+        while (true) {
+            int p = progress[s_prev];
+            if (p >= need) break;
+            if (++it > SPIN_LIMIT || *(volatile int *)err) {
+                atomicExch(err, QD_ERR_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__device__ void publish(int *progress, int s, int val) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(&progress[s], val);
+    }
+}
+
+__global__ void __launch_bounds__(128) hb2st_kernel(double2 *AB, int ldb, int n, int b, int *progress, int *err) {
+    extern __shared__ unsigned char sm_raw[];
+    zd *D = (zd *)sm_raw;        // b x b
+    zd *E = D + b * b;           // b x b
+    zd *v = E + b * b;           // b
+    zd *v2 = v + b;              // b
+    zd *w = v2 + b;              // b
+    __shared__ double scratch[33];
+    __shared__ double s_beta;
+    __shared__ zd s_tau;
+    for (int s = blockIdx.x; s < n - 1; s += gridDim.x) {
+        // ---- task 0: annihilate column s below the subdiagonal
+        if (s > 0 && !wait_progress(progress, s - 1, 3, err)) return;
+        int st = s + 1, ed = min(s + b, n - 1), len = ed - st + 1;
+        for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = ldab(AB, ldb, st + i, s);
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double beta;
+            zd tau;
+            larfg_warp(v, len, &beta, &tau);
+            if (threadIdx.x == 0) { s_beta = beta; s_tau = tau; }
+        }
+        __syncthreads();
+        zd tau = s_tau;
+        for (int i = threadIdx.x; i < len; i += blockDim.x)
+            stab(AB, ldb, st + i, s, i == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0));
+        // diagonal block [st, ed]
+        for (int idx = threadIdx.x; idx < len * len; idx += blockDim.x) {
+            int r = idx % len, c = idx / len;
+            D[r + c * b] = r >= c ? ldab(AB, ldb, st + r, st + c) : cconj(ldab(AB, ldb, st + c, st + r));
+        }
+        __syncthreads();
+        sym_update(D, b, len, v, tau, w, scratch);
+        for (int idx = threadIdx.x; idx < len * len; idx += blockDim.x) {
+            int r = idx % len, c = idx / len;
+            if (r >= c) stab(AB, ldb, st + r, st + c, D[r + c * b]);
+        }
+        publish(progress, s, 1);
+        int k = 1;
+        while (true) {
+            int J1 = ed + 1;
+            if (J1 > n - 1) break;
+            int J2 = min(ed + b, n - 1), lm = J2 - J1 + 1;
+            if (s > 0 && !wait_progress(progress, s - 1, k + 3, err)) return;
+            // E = A[J1..J2, st..ed]
+            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                E[r + c * b] = ldab(AB, ldb, J1 + r, st + c);
+            }
+            __syncthreads();
+            // right application of the previous reflector: E <- E - tau (E v) v^H
+            for (int r = threadIdx.x; r < lm; r += blockDim.x) {
+                zd acc = mk<double>(0, 0);
+                for (int c = 0; c < len; c++) acc = cadd(acc, cmul(E[r + c * b], v[c]));
+                w[r] = cmul(tau, acc);
+            }
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                E[r + c * b] = csub(E[r + c * b], cmul(w[r], cconj(v[c])));
+            }
+            __syncthreads();
+            // new reflector from E[:, 0]
+            for (int i = threadIdx.x; i < lm; i += blockDim.x) v2[i] = E[i];
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                double beta;
+                zd t2;
+                larfg_warp(v2, lm, &beta, &t2);
+                if (threadIdx.x == 0) { s_beta = beta; s_tau = t2; }
+            }
+            __syncthreads();
+            zd tau2 = s_tau;
+            // left application to the remaining columns: E <- E - conj(tau2) v2 (v2^H E)
+            for (int c = 1 + threadIdx.x; c < len; c += blockDim.x) {
+                zd acc = mk<double>(0, 0);
+                for (int r = 0; r < lm; r++) acc = cadd(acc, cmulc(v2[r], E[r + c * b]));
+                w[c] = cmul(cconj(tau2), acc);
+            }
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                zd val;
+                if (c == 0) val = r == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0);
+                else val = csub(E[r + c * b], cmul(v2[r], w[c]));
+                stab(AB, ldb, J1 + r, st + c, val);
+            }
+            __syncthreads();
+            // diagonal block [J1, J2]
+            for (int idx = threadIdx.x; idx < lm * lm; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                D[r + c * b] = r >= c ? ldab(AB, ldb, J1 + r, J1 + c) : cconj(ldab(AB, ldb, J1 + c, J1 + r));
+            }
+            __syncthreads();
+            sym_update(D, b, lm, v2, tau2, w, scratch);
+            for (int idx = threadIdx.x; idx < lm * lm; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                if (r >= c) stab(AB, ldb, J1 + r, J1 + c, D[r + c * b]);
+            }
+            for (int i = threadIdx.x; i < lm; i += blockDim.x) v[i] = v2[i];
+            tau = tau2;
+            st = J1;
+            ed = J2;
+            len = lm;
+            k++;
+            publish(progress, s, k);
+        }
+        publish(progress, s, PROGRESS_DONE);
+        __syncthreads();
+    }
+}
+
+// d[i] = AB(i, i) (real), e[i] = |AB(i+1, i)|^2 (squared off-diagonal moduli)
+__global__ void tri_extract_kernel(const double2 *AB, int ldb, int n, double *d, double *e2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d[i] = AB[(int64_t)i * ldb].x;
+    if (i < n - 1) {
+        double2 e = AB[1 + (int64_t)i * ldb];
+        e2[i] = e.x * e.x + e.y * e.y;
+    }
+}
+
+// Gershgorin bounds and the pivot floor (LAPACK dlaebz/dstebz conventions)
+__global__ void gersh_kernel(const double *d, const double *e2, int n, double *out /*gl, gu, pivmin*/) {
+    double gl = 1e300, gu = -1e300, emax = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double r = (i > 0 ? sqrt(e2[i - 1]) : 0.0) + (i < n - 1 ? sqrt(e2[i]) : 0.0);
+        gl = fmin(gl, d[i] - r);
+        gu = fmax(gu, d[i] + r);
+        if (i < n - 1) emax = fmax(emax, e2[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gl = fmin(gl, __shfl_xor_sync(0xffffffffu, gl, o));
+        gu = fmax(gu, __shfl_xor_sync(0xffffffffu, gu, o));
+        emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    }
+    __shared__ double sg[3][32];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sg[0][w] = gl; sg[1][w] = gu; sg[2][w] = emax; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); q++) {
+            gl = fmin(gl, sg[0][q]); gu = fmax(gu, sg[1][q]); emax = fmax(emax, sg[2][q]);
+        }
+        double tnorm = fmax(fabs(gl), fabs(gu));
+        double pad = 2.1 * 2.220446049250313e-16 * tnorm * n;
+        out[0] = gl - pad;
+        out[1] = gu + pad;
+        out[2] = 2.2250738585072014e-308 * fmax(1.0, emax);
+    }
+}
+
+__device__ int sturm_count(const double *d, const double *e2, int n, double x, double pivmin) {
+    int c = 0;
+    double q = d[0] - x;
+    if (fabs(q) <= pivmin) q = -pivmin;
+    c += q < 0.0;
+    for (int i = 1; i < n; i++) {
+        q = d[i] - x - e2[i - 1] / q;
+        if (fabs(q) <= pivmin) q = -pivmin;
+        c += q < 0.0;
+    }
+    return c;
+}
+
+// One warp per wanted index k in [lo, hi]: interval [a, b] with count(a) <= k < count(b).
+__global__ void bisect_kernel(const double *d, const double *e2, int n, int lo, int hi, const double *bounds,
+                              double *w) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int k = lo + warp;
+    if (k > hi) return;
+    double a = bounds[0], bnd = bounds[1], pivmin = bounds[2];
+    for (int it = 0; it < 64; it++) {
+        double width = bnd - a;
+        double tol = 2.0 * 2.220446049250313e-16 * fmax(fabs(a), fabs(bnd)) + 4.0 * pivmin;
+        if (width <= tol) break;
+        double x = a + width * (double)(lane + 1) / 33.0;
+        int c = sturm_count(d, e2, n, x, pivmin);
+        unsigned above = __ballot_sync(0xffffffffu, c > k);
+        int first = above ? __ffs(above) - 1 : 32;  // smallest lane with count > k
+        double na = first == 0 ? a : a + width * (double)first / 33.0;
+        double nb = first == 32 ? bnd : a + width * (double)(first + 1) / 33.0;
+        a = na;
+        bnd = nb;
+    }
+    if (lane == 0) w[k - lo] = 0.5 * (a + bnd);
+}
+
+// ---------------------------------------------------------------------------
+// Band inverse iteration.  One block per group of degenerate eigenvalues.
+// B is the Hermitian band before stage 2 (AB0, lower, offsets 0..b, ldb).
+// Workspace per group: L (n x b), U (n x (2b+1)), ipiv (n).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ zd band_val(const double2 *AB, int ldb, int b, int n, int64_t i, int64_t c, double lam) {
+    if (i < 0 || c < 0 || i >= n || c >= n) return mk<double>(0, 0);
+    int64_t d = i - c;
+    zd v;
+    if (d >= 0) {
+        if (d > b) return mk<double>(0, 0);
+        double2 x = AB[d + c * (int64_t)ldb];
+        v = mk<double>(x.x, x.y);
+    } else {
+        if (-d > b) return mk<double>(0, 0);
+        double2 x = AB[-d + i * (int64_t)ldb];
+        v = mk<double>(x.x, -x.y);
+    }
+    if (d == 0) v.re -= lam;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int ldb, int n, int b, const double *lam,
+                                                         const int *group_start, const int *group_size, double2 *Lw,
+                                                         double2 *Uw, int *ipivw, double2 *Z, int64_t ldz,
+                                                         double bnorm, double2 *ywork) {
+    extern __shared__ unsigned char sm_raw[];
+    const int rows = b + 1, cols = 2 * b + 1;
+    zd *W = (zd *)sm_raw;                 // [rows][cols] circular window
+    zd *lcol = W + rows * cols;           // b multipliers of the current step
+    __shared__ double scratch[33];
+    __shared__ int s_piv;
+    __shared__ zd s_inv;
+    int g = blockIdx.x;
+    int m0 = group_start[g], gs = group_size[g];
+    double lambda = lam[m0];
+    double2 *L = Lw + (int64_t)g * n * b;
+    double2 *U = Uw + (int64_t)g * n * cols;
+    int *ipiv = ipivw + (int64_t)g * n;
+    // window slot of (i, c): W[(i % rows) * cols + (c % cols)]
+    for (int idx = threadIdx.x; idx < rows * cols; idx += blockDim.x) {
+        int i = idx / cols, c = idx % cols;
+        W[(i % rows) * cols + (c % cols)] = band_val(AB, ldb, b, n, i, c, lambda);
+    }
+    __syncthreads();
+    const double tiny = 2.220446049250313e-16 * bnorm;
+    for (int j = 0; j < n; j++) {
+        int imax = min(j + b, n - 1), cmax = min(j + 2 * b, n - 1);
+        if (threadIdx.x < 32) {
+            // pivot search in column j, rows j..imax
+            double best = -1.0;
+            int bi = j;
+            for (int i = j + threadIdx.x; i <= imax; i += 32) {
+                double a = cabs2(W[(i % rows) * cols + (j % cols)]);
+                if (a > best) { best = a; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (threadIdx.x == 0) s_piv = bi;
+            __syncwarp();
+            int p = bi;
+            if (p != j) {
+                for (int c = j + threadIdx.x; c <= cmax; c += 32) {
+                    zd t = W[(j % rows) * cols + (c % cols)];
+                    W[(j % rows) * cols + (c % cols)] = W[(p % rows) * cols + (c % cols)];
+                    W[(p % rows) * cols + (c % cols)] = t;
+                }
+            }
+            __syncwarp();
+            if (threadIdx.x == 0) {
+                zd piv = W[(j % rows) * cols + (j % cols)];
+                double a2 = cabs2(piv);
+                if (a2 < tiny * tiny) {
+                    piv = mk<double>(tiny, 0.0);
+                    W[(j % rows) * cols + (j % cols)] = piv;
+                    a2 = tiny * tiny;
+                }
+                s_inv = mk<double>(piv.re / a2, -piv.im / a2);
+            }
+            __syncwarp();
+            for (int i = j + 1 + threadIdx.x; i <= imax; i += 32) {
+                zd l = cmul(W[(i % rows) * cols + (j % cols)], s_inv);
+                lcol[i - j - 1] = l;
+                L[(int64_t)j * b + (i - j - 1)] = make_double2(l.re, l.im);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) ipiv[j] = s_piv;
+        // U row j and the rank-1 update of the trailing window
+        for (int c = j + threadIdx.x; c < j + cols; c += blockDim.x) {
+            zd u = c <= cmax ? W[(j % rows) * cols + (c % cols)] : mk<double>(0, 0);
+            U[(int64_t)j * cols + (c - j)] = make_double2(u.re, u.im);
+        }
+        int nr = imax - j, nc = cmax - j;
+        for (int idx = threadIdx.x; idx < nr * nc; idx += blockDim.x) {
+            int i = j + 1 + idx % nr, c = j + 1 + idx / nr;
+            zd *a = &W[(i % rows) * cols + (c % cols)];
+            *a = csub(*a, cmul(lcol[i - j - 1], W[(j % rows) * cols + (c % cols)]));
+        }
+        __syncthreads();
+        // slide the window: row j leaves (slot reused by row j+b+1), column j leaves (slot for j+2b+1)
+        int nrow = j + b + 1, ncol = j + 2 * b + 1;
+        for (int c = j + 1 + threadIdx.x; c <= j + 2 * b + 1; c += blockDim.x)
+            W[(nrow % rows) * cols + (c % cols)] = band_val(AB, ldb, b, n, nrow, c, lambda);
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < j + b + 1; i += blockDim.x)
+            W[(i % rows) * cols + (ncol % cols)] = band_val(AB, ldb, b, n, i, ncol, lambda);
+        __syncthreads();
+    }
+    // ---- inverse iteration on the group's block of vectors (one warp per vector).
+    // The forward and backward sweeps keep their active windows (b+1 and 2b+1
+    // entries) in per-warp circular buffers in shared memory.
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    zd *fb = lcol + b + warp * 192;  // 64 slots forward window
+    zd *bb = fb + 64;                // 128 slots backward window
+    for (int it = 0; it < 3; it++) {
+        for (int q = warp; q < gs; q += nwarp) {
+            double2 *y = ywork + ((int64_t)blockIdx.x * 8 + warp) * n;
+            double2 *x = Z + (int64_t)(m0 + q) * ldz;
+            auto rhs = [&](int i) -> zd {
+                if (it == 0) {
+                    unsigned h = (unsigned)(i * 2654435761u) ^ (unsigned)((m0 + q + 1) * 40503u);
+                    h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+                    unsigned h2 = h * 2246822519u + 374761393u;
+                    return mk<double>((double)(h & 0xffff) / 65536.0 - 0.5, (double)(h2 & 0xffff) / 65536.0 - 0.5);
+                }
+                double2 t = x[i];
+                return mk<double>(t.x, t.y);
+            };
+            for (int i = lane; i <= b && i < n; i += 32) fb[i & 63] = rhs(i);
+            __syncwarp();
+            // forward: P and L
+            for (int j = 0; j < n; j++) {
+                int p = ipiv[j];
+                if (lane == 0 && p != j) {
+                    zd t = fb[j & 63];
+                    fb[j & 63] = fb[p & 63];
+                    fb[p & 63] = t;
+                }
+                __syncwarp();
+                zd yj = fb[j & 63];
+                int i = j + 1 + lane;
+                if (lane < b && i < n) {
+                    double2 l = L[(int64_t)j * b + lane];
+                    fb[i & 63] = csub(fb[i & 63], cmul(mk<double>(l.x, l.y), yj));
+                }
+                if (lane == 0) y[j] = make_double2(yj.re, yj.im);
+                if (lane == 1 && j + b + 1 < n) fb[(j + b + 1) & 63] = rhs(j + b + 1);
+                __syncwarp();
+            }
+            // backward: U x = y
+            for (int j = n - 1; j >= 0; j--) {
+                double sr = 0.0, si = 0.0;
+                int cend = min(j + 2 * b, n - 1);
+                for (int c = j + 1 + lane; c <= cend; c += 32) {
+                    double2 u = U[(int64_t)j * cols + (c - j)];
+                    zd xc = bb[c & 127];
+                    sr += u.x * xc.re - u.y * xc.im;
+                    si += u.x * xc.im + u.y * xc.re;
+                }
+                sr = warp_sum(sr);
+                si = warp_sum(si);
+                if (lane == 0) {
+                    double2 u = U[(int64_t)j * cols];
+                    double2 yy = y[j];
+                    double rr = yy.x - sr, ri = yy.y - si;
+                    double den = u.x * u.x + u.y * u.y;
+                    zd xj = mk<double>((rr * u.x + ri * u.y) / den, (ri * u.x - rr * u.y) / den);
+                    bb[j & 127] = xj;
+                    x[j] = make_double2(xj.re, xj.im);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // modified Gram-Schmidt within the group (block-wide reductions)
+        for (int q = 0; q < gs; q++) {
+            double2 *xq = Z + (int64_t)(m0 + q) * ldz;
+            for (int p = 0; p < q; p++) {
+                double2 *xp = Z + (int64_t)(m0 + p) * ldz;
+                double sr = 0.0, si = 0.0;
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    double2 a = xp[i], c = xq[i];
+                    sr += a.x * c.x + a.y * c.y;
+                    si += a.x * c.y - a.y * c.x;
+                }
+                sr = block_sum(sr, scratch);
+                si = block_sum(si, scratch);
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    double2 a = xp[i], c = xq[i];
+                    c.x -= sr * a.x - si * a.y;
+                    c.y -= sr * a.y + si * a.x;
+                    xq[i] = c;
+                }
+                __syncthreads();
+            }
+            double nn = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) nn += xq[i].x * xq[i].x + xq[i].y * xq[i].y;
+            nn = block_sum(nn, scratch);
+            double inv = nn > 0.0 ? 1.0 / sqrt(nn) : 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) xq[i] = make_double2(xq[i].x * inv, xq[i].y * inv);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host wrappers
+// ---------------------------------------------------------------------------
+#define CUDA_OK(x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess)                                                                        \
+            return qd_set_error(QD_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *err, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t smem = (size_t)(2 * b * b + 3 * b) * sizeof(zd);
+    CUDA_OK(cudaFuncSetAttribute(hb2st_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev, nsm, per_sm = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 128, smem));
+    if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
+    int G = nsm * per_sm;
+    int useful = n / (2 * b) + 2;  // concurrent sweeps are limited by the 3-task lag
+    if (G > useful) G = useful;
+    if (G > n - 1) G = n - 1;
+    if (G < 1) G = 1;
+    CUDA_OK(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n, st));
+    CUDA_OK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    void *args[] = {&AB, &ldb, &n, &b, &progress, &err};
+    CUDA_OK(cudaLaunchCooperativeKernel((void *)hb2st_kernel, dim3(G), dim3(128), args, smem, st));
+    return QD_OK;
+}
+
+extern "C" int qd_tridiag_bisect(const double2 *AB, int ldb, int n, int lo, int hi, double *d, double *e2,
+                                 double *bounds, double *w, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    tri_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(AB, ldb, n, d, e2);
+    gersh_kernel<<<1, 1024, 0, st>>>(d, e2, n, bounds);
+    int m = hi - lo + 1;
+    bisect_kernel<<<(m * 32 + 127) / 128, 128, 0, st>>>(d, e2, n, lo, hi, bounds, w);
+    CUDA_OK(cudaGetLastError());
+    return QD_OK;
+}
+
+extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const double *lam_dev, int ngroups,
+                             const int *gstart_dev, const int *gsize_dev, double2 *Lw, double2 *Uw, int *ipivw,
+                             double2 *Z, int64_t ldz, double bnorm, double2 *ywork, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t smem = (size_t)((b + 1) * (2 * b + 1) + b + 8 * 192) * sizeof(zd);
+    CUDA_OK(cudaFuncSetAttribute(band_invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    band_invit_kernel<<<ngroups, 256, smem, st>>>(AB0, ldb, n, b, lam_dev, gstart_dev, gsize_dev, Lw, Uw, ipivw, Z,
+                                                  ldz, bnorm, ywork);
+    CUDA_OK(cudaGetLastError());
+    return QD_OK;
+}

@@ -1,0 +1,522 @@
+/* C entry points of libqdgpu: error state, problem set-up from the reference's
+ * input files, the status-returning qd_* API and the reference-named routines
+ * (hamiltonian_8_band, diagonalise_hamiltonian, eigenstates,
+ * coulomb_matrix_elements) with the reference's global state. */
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <dlfcn.h>
+
+#include <cublas_v2.h>
+#include <cuda_runtime_api.h>
+
+#include "qd_internal.h"
+
+/* ------------------------------------------------------------------------- */
+/* Reference global state (8_band_main.c:36-65).  Weak, so that the           */
+/* reference's own definitions win when its main program links this library. */
+/* ------------------------------------------------------------------------- */
+#define QD_WEAK __attribute__((weak))
+QD_WEAK int N_shape = 0;
+QD_WEAK int isotropic = 0;
+QD_WEAK int softening = 0;
+QD_WEAK int include_strain = 0;
+QD_WEAK int include_piezo = 0;
+QD_WEAK int include_CME = 0;
+QD_WEAK int PACKED = 0;
+QD_WEAK int myid = 0;
+QD_WEAK int nprocs = 1;
+QD_WEAK int64_t N_H = 0, na_rows = 0, na_cols = 0, na_rowsz = 0, na_colsz = 0, np_rows = 1, np_cols = 1, my_prow = 0,
+                my_pcol = 0, block_size = 0;
+QD_WEAK struct characteristic_functions *characteristic_function_G = NULL;
+QD_WEAK struct strain_tensor strain_G = {0};
+QD_WEAK struct convolution_char_strain *convolutions_char_strain = NULL;
+QD_WEAK struct piezo_potential phi_piezo_G = {0};
+QD_WEAK struct timing component_run_times = {0};
+
+/* ------------------------------------------------------------------------- */
+/* errors                                                                    */
+/* ------------------------------------------------------------------------- */
+static __thread char g_err[512];
+static __thread int g_err_code;
+
+int qd_set_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    g_err_code = code;
+    return code;
+}
+
+const char *qd_last_error_message(void) { return g_err; }
+int qd_version(void) { return 1; }
+
+/* Device-memory, copy and event helpers so that callers without a CUDA
+ * toolkit binding (ctypes, Fortran, ...) can drive the device-resident entry
+ * points. */
+int qd_dev_alloc(size_t bytes, void **out) {
+    cudaError_t e = cudaMalloc(out, bytes ? bytes : 16);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_dev_free(void *p) {
+    if (p) cudaFree(p);
+    return QD_OK;
+}
+int qd_memcpy(void *dst, const void *src, size_t bytes, int kind) {
+    /* kind: 1 host->device, 2 device->host, 3 device->device */
+    enum cudaMemcpyKind k = kind == 1 ? cudaMemcpyHostToDevice : kind == 2 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaMemcpy(dst, src, bytes, k);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_memset(void *dst, int value, size_t bytes) {
+    cudaError_t e = cudaMemset(dst, value, bytes);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_host_alloc_pinned(size_t bytes, void **out) {
+    cudaError_t e = cudaMallocHost(out, bytes ? bytes : 16);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_NOMEM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_host_free_pinned(void *p) {
+    if (p) cudaFreeHost(p);
+    return QD_OK;
+}
+int qd_device_synchronize(void) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "device: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_device_count(int *n) {
+    cudaError_t e = cudaGetDeviceCount(n);
+    if (e != cudaSuccess) {
+        *n = 0;
+        return qd_set_error(QD_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    return QD_OK;
+}
+int qd_set_device(int dev) {
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_event_create(void **ev) {
+    cudaError_t e = cudaEventCreate((cudaEvent_t *)ev);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaEventCreate: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_event_record(void *ev, void *stream) {
+    cudaError_t e = cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaEventRecord: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_event_elapsed_ms(void *ev0, void *ev1, float *ms) {
+    cudaError_t e = cudaEventSynchronize((cudaEvent_t)ev1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, (cudaEvent_t)ev0, (cudaEvent_t)ev1);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "cudaEventElapsedTime: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+int qd_event_destroy(void *ev) {
+    if (ev) cudaEventDestroy((cudaEvent_t)ev);
+    return QD_OK;
+}
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess)                                                                  \
+            return qd_set_error(QD_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    } while (0)
+#define RC(x)                         \
+    do {                              \
+        int rc_ = (x);                \
+        if (rc_ != QD_OK) return rc_; \
+    } while (0)
+
+static cublasHandle_t g_cublas = NULL;
+cublasHandle_t qd_cublas(void) {
+    if (!g_cublas) {
+        cublasCreate(&g_cublas);
+        /* FP32 emulation on the tensor cores needs cuBLAS >= 12.9; looked up at run
+         * time so that an older cuBLAS already loaded in the process still works
+         * (the complex64 products then run in plain FP32). */
+        typedef cublasStatus_t (*set_strategy_fn)(cublasHandle_t, int);
+        set_strategy_fn f = (set_strategy_fn)dlsym(RTLD_DEFAULT, "cublasSetEmulationStrategy");
+        if (f) f(g_cublas, 2 /* CUBLAS_EMULATION_STRATEGY_EAGER */);
+    }
+    return g_cublas;
+}
+
+/* complex64 GEMM arithmetic of the mixed path: 2 = FP32 emulated with BF16x9 on
+ * the tensor cores (default), 1 = TF32, 0 = plain FP32.  QD_MIXED_GEMM overrides. */
+int qd_mixed_gemm_mode(void) {
+    const char *s = getenv("QD_MIXED_GEMM");
+    return s ? atoi(s) : 2;
+}
+
+void qd_set_timing(int i, double ms);
+
+/* ------------------------------------------------------------------------- */
+/* problem set-up                                                            */
+/* ------------------------------------------------------------------------- */
+static char *read_file(const char *dir, const char *name) {
+    char path[4096];
+    snprintf(path, sizeof(path), "%s/%s", dir, name);
+    FILE *f = fopen(path, "rb");
+    if (!f) return NULL;
+    fseek(f, 0, SEEK_END);
+    long n = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    char *buf = (char *)malloc((size_t)n + 1);
+    if (buf && fread(buf, 1, (size_t)n, f) != (size_t)n) {
+        free(buf);
+        buf = NULL;
+    }
+    if (buf) buf[n] = 0;
+    fclose(f);
+    return buf;
+}
+
+static int setup_problem(struct qd_problem *pr) {
+    qd_params *p = &pr->p;
+    if (p->n_shape < 1) return qd_set_error(QD_ERR_INPUT, "N_shape must be >= 1");
+    for (int a = 0; a < 3; a++)
+        if (p->N[a] < 1) return qd_set_error(QD_ERR_INPUT, "number of plane waves must be >= 1");
+    struct supercell_geometry *g0 = &pr->geo[0];
+    double L[3] = {g0->L1, g0->L2, g0->L3}, SL[3] = {g0->SL1, g0->SL2, g0->SL3};
+    /* 8_band_main.c:195-200 */
+    if (p->strain_type == 1 && g0->RL1 == 1 && g0->RL2 == 1 && g0->RL3 == 1 && p->N[0] == p->NS[0] &&
+        p->N[1] == p->NS[1] && p->N[2] == p->NS[2])
+        p->strain_type = 0;
+    RC(qd_material_parameters(p->T, p->piezo, p->n_shape, pr->geo, pr->mat));
+    pr->nT = 1;
+    pr->nTS = 1;
+    pr->n_pw = 1;
+    for (int a = 0; a < 3; a++) {
+        pr->NT[a] = 2 * p->N[a] - 1;
+        pr->nT *= pr->NT[a];
+        pr->n_pw *= p->N[a];
+        pr->G[a] = (double *)malloc(sizeof(double) * pr->NT[a]);
+        qd_basis_grid(pr->NT[a], L[a], pr->G[a]);
+        if (p->strain) {
+            pr->NTS[a] = 2 * p->NS[a] - 1;
+            pr->nTS *= pr->NTS[a];
+            pr->GS[a] = (double *)malloc(sizeof(double) * pr->NTS[a]);
+            qd_basis_grid(pr->NTS[a], SL[a], pr->GS[a]);
+        }
+    }
+    pr->n_h = 8 * pr->n_pw;
+    pr->same_cells = p->strain && p->N[0] == p->NS[0] && p->N[1] == p->NS[1] && p->N[2] == p->NS[2] && L[0] == SL[0] &&
+                     L[1] == SL[1] && L[2] == SL[2];
+    /* eigenstates.c:29-36 (0-based) */
+    int idx_cb_min = (QD_N_BAND - 2) * (int)pr->n_pw;
+    pr->lo = idx_cb_min - 2 * p->n_vb;
+    pr->hi = idx_cb_min + 2 * p->n_cb - 1;
+    if (pr->lo < 0 || pr->hi >= pr->n_h || pr->lo > pr->hi)
+        return qd_set_error(QD_ERR_INPUT, "eigenstate window outside the spectrum");
+    return QD_OK;
+}
+
+int qd_problem_load(const char *dir, const char *const *overrides, int n_overrides, qd_problem **out) {
+    *out = NULL;
+    char *ptext = read_file(dir, "parameters.in");
+    if (!ptext) return qd_set_error(QD_ERR_INPUT, "Error. Failed to open parameters.in file.");
+    struct qd_problem *pr = (struct qd_problem *)calloc(1, sizeof(struct qd_problem));
+    int rc = qd_read_parameters_text(ptext, &pr->p, NULL);
+    free(ptext);
+    for (int i = 0; rc == QD_OK && i < n_overrides; i++) rc = qd_apply_override(&pr->p, overrides[i]);
+    if (rc) {
+        free(pr);
+        return rc;
+    }
+    char *stext = read_file(dir, "supercell.in");
+    if (!stext) {
+        free(pr);
+        return qd_set_error(QD_ERR_INPUT, "Error. Failed to open supercell.in file.");
+    }
+    pr->geo = (struct supercell_geometry *)calloc((size_t)pr->p.n_shape, sizeof(struct supercell_geometry));
+    pr->mat = (struct material_params *)calloc((size_t)pr->p.n_shape, sizeof(struct material_params));
+    rc = qd_read_supercell_text(stext, &pr->p, pr->geo);
+    free(stext);
+    if (rc == QD_OK) rc = setup_problem(pr);
+    if (rc) {
+        qd_problem_free(pr);
+        return rc;
+    }
+    *out = pr;
+    return QD_OK;
+}
+
+void qd_problem_free(qd_problem *pr) {
+    if (!pr) return;
+    for (int a = 0; a < 3; a++) {
+        free(pr->G[a]);
+        free(pr->GS[a]);
+        if (pr->d_G[a]) cudaFree(pr->d_G[a]);
+        if (pr->d_GS[a]) cudaFree(pr->d_GS[a]);
+    }
+    void *dev[] = {pr->d_geo, pr->d_mat, pr->d_chi_s, pr->d_eps_s, pr->d_phi_s, pr->d_chi,
+                   pr->d_eps, pr->d_phi, pr->d_conv, pr->d_coef};
+    for (size_t i = 0; i < sizeof(dev) / sizeof(dev[0]); i++)
+        if (dev[i]) cudaFree(dev[i]);
+    free(pr->geo);
+    free(pr->mat);
+    free(pr);
+}
+
+int qd_problem_sizes(const qd_problem *pr, int64_t *n_pw, int64_t *n_h, int *lo, int *hi, int *n_vb, int *n_cb) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    if (n_pw) *n_pw = pr->n_pw;
+    if (n_h) *n_h = pr->n_h;
+    if (lo) *lo = pr->lo;
+    if (hi) *hi = pr->hi;
+    if (n_vb) *n_vb = pr->p.n_vb;
+    if (n_cb) *n_cb = pr->p.n_cb;
+    return QD_OK;
+}
+
+int qd_problem_materials(const qd_problem *pr, struct material_params *out, int n) {
+    if (!pr || n != pr->p.n_shape) return qd_set_error(QD_ERR_ARG, "n_shape mismatch");
+    memcpy(out, pr->mat, sizeof(*out) * (size_t)n);
+    return QD_OK;
+}
+
+int qd_problem_geometry(const qd_problem *pr, struct supercell_geometry *out, int n) {
+    if (!pr || n != pr->p.n_shape) return qd_set_error(QD_ERR_ARG, "n_shape mismatch");
+    memcpy(out, pr->geo, sizeof(*out) * (size_t)n);
+    return QD_OK;
+}
+
+int qd_problem_build_tables(qd_problem *pr) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    if (pr->tables_ready) return QD_OK;
+    return qd_tables_build_dev(pr);
+}
+
+int qd_problem_get_table(const qd_problem *pr, int which, int s, int c, qd_complex128 *out, int64_t n) {
+    if (!pr || !pr->tables_ready) return qd_set_error(QD_ERR_ARG, "tables not built");
+    const void *src = NULL;
+    int64_t nt = (which >= 4) ? pr->nTS : pr->nT;
+    if (n != nt) return qd_set_error(QD_ERR_ARG, "table size %lld != %lld", (long long)n, (long long)nt);
+    int ns = pr->p.n_shape;
+    switch (which) {
+        case 0: if (s < 1 || s >= ns) break; src = (const qd_complex128 *)pr->d_chi + (int64_t)s * nt; break;
+        case 1: if (!pr->d_eps || s < 0 || s > 5) break; src = (const qd_complex128 *)pr->d_eps + (int64_t)s * nt; break;
+        case 2: src = pr->d_phi; break;
+        case 3: if (!pr->d_conv || s < 1 || s >= ns || c < 0 || c > 7) break;
+            src = (const qd_complex128 *)pr->d_conv + ((int64_t)s * 8 + c) * nt; break;
+        case 4: if (!pr->d_chi_s || s < 1 || s >= ns) break; src = (const qd_complex128 *)pr->d_chi_s + (int64_t)s * nt; break;
+        case 5: if (!pr->d_eps_s || s < 0 || s > 5) break; src = (const qd_complex128 *)pr->d_eps_s + (int64_t)s * nt; break;
+        case 6: src = pr->d_phi_s; break;
+        case 7: if (c < 0 || c >= QD_N_COEF) break; src = (const qd_complex128 *)pr->d_coef + (int64_t)c * nt; break;
+        default: break;
+    }
+    if (!src) return qd_set_error(QD_ERR_ARG, "table (%d, %d, %d) not available", which, s, c);
+    CK(cudaMemcpy(out, src, sizeof(qd_complex128) * (size_t)nt, cudaMemcpyDeviceToHost));
+    return QD_OK;
+}
+
+int qd_problem_assemble_dev(qd_problem *pr, void *H_dev, int64_t ld, int mode, int prec, void *stream) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    RC(qd_problem_build_tables(pr));
+    return qd_assemble_launch(pr->d_coef, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, H_dev, ld, mode, prec,
+                              stream);
+}
+
+int qd_eigh_window_dev(int64_t n, void *H_dev, int64_t ld, int lo, int hi, int prec, double *eigval_dev,
+                       void *eigvec_dev, int64_t ldz, void *stream) {
+    return qd_eigh_window(n, H_dev, ld, lo, hi, prec, eigval_dev, eigvec_dev, ldz, stream);
+}
+
+int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *eigvec) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    RC(qd_problem_build_tables(pr));
+    int64_t n = pr->n_h;
+    int M = pr->hi - pr->lo + 1;
+    void *H = NULL, *Z = NULL;
+    double *w = NULL;
+    CK(cudaMalloc(&H, sizeof(qd_complex128) * (size_t)n * (size_t)n));
+    CK(cudaMalloc(&Z, sizeof(qd_complex128) * (size_t)n * (size_t)M));
+    CK(cudaMalloc((void **)&w, sizeof(double) * (size_t)M));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    int rc = qd_problem_assemble_dev(pr, H, n, 0, QD_PREC_FP64, NULL);
+    cudaEventRecord(e1, 0);
+    if (rc == QD_OK) rc = qd_eigh_window(n, H, n, pr->lo, pr->hi, prec, w, Z, n, NULL);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    qd_set_timing(0, ms);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == QD_OK) {
+        cudaError_t e = cudaMemcpy(eigval, w, sizeof(double) * (size_t)M, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(eigvec, Z, sizeof(qd_complex128) * (size_t)n * (size_t)M, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "copy-out: %s", cudaGetErrorString(e));
+    }
+    cudaFree(H);
+    cudaFree(Z);
+    cudaFree(w);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Reference-named routines                                                  */
+/* ------------------------------------------------------------------------- */
+static double wall_s(void) {
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+static int env_precision(void) {
+    const char *s = getenv("QD_PRECISION");
+    return (s && (!strcmp(s, "mixed") || !strcmp(s, "1"))) ? QD_PREC_MIXED : QD_PREC_FP64;
+}
+
+static void die(const char *where, int rc) {
+    /* The reference prints a message and aborts (diagonalise_hamiltonian.c:279-293). */
+    printf("%s failed (%d): %s\n", where, rc, qd_last_error_message());
+    fflush(stdout);
+    exit(1);
+}
+
+static int check_single_rank(void) {
+    if (nprocs != 1 || PACKED)
+        return qd_set_error(QD_ERR_UNSUPPORTED, "the GPU solve path runs as a single process with PACKED = 0");
+    return QD_OK;
+}
+
+/* Uploads the reference's global tables, fuses them and assembles H on the device. */
+static int assemble_from_globals(int n_shape, struct vector F, struct wave_vectors basis,
+                                 struct supercell_geometry *supercell, struct material_params *parameters, void *H_dev,
+                                 int64_t ld) {
+    int N[3] = {basis.N_Gx, basis.N_Gy, basis.N_Gz};
+    const qd_complex128 *chi[1024];
+    const qd_complex128 *eps[6];
+    const qd_complex128 **conv8 = NULL;
+    if (n_shape > 1024) return qd_set_error(QD_ERR_UNSUPPORTED, "more than 1024 shapes");
+    chi[0] = NULL;
+    for (int s = 1; s < n_shape; s++) chi[s] = characteristic_function_G[s].chi;
+    int strain_on = include_strain != 0;
+    int piezo_on = strain_on && include_piezo != 0;
+    if (strain_on) {
+        eps[0] = strain_G.xx; eps[1] = strain_G.yy; eps[2] = strain_G.zz;
+        eps[3] = strain_G.yz; eps[4] = strain_G.xz; eps[5] = strain_G.xy;
+        conv8 = (const qd_complex128 **)calloc((size_t)n_shape * 8, sizeof(*conv8));
+        for (int s = 1; s < n_shape; s++) {
+            const struct convolution_char_strain *c = &convolutions_char_strain[s];
+            conv8[s * 8 + 0] = c->char_xx; conv8[s * 8 + 1] = c->char_yy; conv8[s * 8 + 2] = c->char_zz;
+            conv8[s * 8 + 3] = c->char_yz; conv8[s * 8 + 4] = c->char_xz; conv8[s * 8 + 5] = c->char_xy;
+            conv8[s * 8 + 6] = c->char_hydrostatic; conv8[s * 8 + 7] = c->char_biaxial;
+        }
+    }
+    double Fv[3] = {F.x, F.y, F.z};
+    void *d_coef = NULL;
+    double *d_G = NULL;
+    int rc = qd_coef_from_host_tables(n_shape, N, basis.Gx, basis.Gy, basis.Gz, basis.Kx, basis.Ky, basis.Kz, Fv,
+                                      supercell, parameters, strain_on, piezo_on, chi, eps,
+                                      piezo_on ? phi_piezo_G.pz : NULL, conv8, &d_coef, &d_G);
+    free(conv8);
+    if (rc) return rc;
+    int NT[3] = {2 * N[0] - 1, 2 * N[1] - 1, 2 * N[2] - 1};
+    double K[3] = {basis.Kx, basis.Ky, basis.Kz};
+    rc = qd_assemble_launch(d_coef, d_G, d_G + NT[0], d_G + NT[0] + NT[1], N, K, H_dev, ld, 0, QD_PREC_FP64, NULL);
+    if (rc == QD_OK && cudaDeviceSynchronize() != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "assembly failed");
+    cudaFree(d_coef);
+    cudaFree(d_G);
+    return rc;
+}
+
+void hamiltonian_8_band(int n_shape, struct vector F, struct wave_vectors basis, struct supercell_geometry *supercell,
+                        struct material_params *parameters, qd_complex128 *H) {
+    int rc = check_single_rank();
+    int64_t n = (int64_t)8 * basis.N_Gx * basis.N_Gy * basis.N_Gz;
+    int64_t ld = na_rows > 0 ? na_rows : n;
+    void *Hd = NULL;
+    if (rc == QD_OK && cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_NOMEM, "device H");
+    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, ld);
+    /* copy the lower triangle column by column; the caller's strict upper triangle is left as it was */
+    for (int64_t c = 0; rc == QD_OK && c < n; c++) {
+        cudaError_t e = cudaMemcpy(H + c + c * ld, (qd_complex128 *)Hd + c + c * ld, sizeof(qd_complex128) * (size_t)(n - c),
+                                   cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "copy-out: %s", cudaGetErrorString(e));
+    }
+    if (Hd) cudaFree(Hd);
+    if (rc) die("hamiltonian_8_band", rc);
+}
+
+void diagonalise_hamiltonian(int *idx_eig, qd_complex128 *H, double *eigval, qd_complex128 *eigvec) {
+    int rc = check_single_rank();
+    int64_t n = N_H;
+    int64_t ld = na_rows > 0 ? na_rows : n;
+    int lo = idx_eig[0] - 1, hi = idx_eig[1] - 1, M = hi - lo + 1;
+    void *Hd = NULL, *Zd = NULL;
+    double *wd = NULL;
+    if (rc == QD_OK && (cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n) != cudaSuccess ||
+                        cudaMalloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M) != cudaSuccess ||
+                        cudaMalloc((void **)&wd, sizeof(double) * (size_t)M) != cudaSuccess))
+        rc = qd_set_error(QD_ERR_NOMEM, "device buffers");
+    if (rc == QD_OK && cudaMemcpy(Hd, H, sizeof(qd_complex128) * (size_t)ld * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "copy-in");
+    if (rc == QD_OK) rc = qd_eigh_window(n, Hd, ld, lo, hi, env_precision(), wd, Zd, n, NULL);
+    if (rc == QD_OK && (cudaMemcpy(eigval, wd, sizeof(double) * (size_t)M, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(eigvec, Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M, cudaMemcpyDeviceToHost) != cudaSuccess))
+        rc = qd_set_error(QD_ERR_CUDA, "copy-out");
+    cudaFree(Hd);
+    cudaFree(Zd);
+    cudaFree(wd);
+    if (rc) die("diagonalise_hamiltonian", rc);
+}
+
+void eigenstates(int n_shape, int *N_states, struct vector F, struct wave_vectors basis,
+                 struct supercell_geometry *supercell, struct material_params *parameters,
+                 struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb) {
+    int rc = check_single_rank();
+    int64_t npw = (int64_t)basis.N_Gx * basis.N_Gy * basis.N_Gz, n = 8 * npw;
+    int idx_cb_min = (QD_N_BAND - 2) * (int)npw; /* eigenstates.c:29-36 */
+    int lo = idx_cb_min - 2 * N_states[0], hi = idx_cb_min + 2 * N_states[1] - 1, M = hi - lo + 1;
+    void *Hd = NULL, *Zd = NULL;
+    double *wd = NULL;
+    if (rc == QD_OK && (cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)n * (size_t)n) != cudaSuccess ||
+                        cudaMalloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M) != cudaSuccess ||
+                        cudaMalloc((void **)&wd, sizeof(double) * (size_t)M) != cudaSuccess))
+        rc = qd_set_error(QD_ERR_NOMEM, "device buffers");
+    double t0 = wall_s();
+    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, n);
+    double t1 = wall_s();
+    if (rc == QD_OK) rc = qd_eigh_window(n, Hd, n, lo, hi, env_precision(), wd, Zd, n, NULL);
+    double t2 = wall_s();
+    component_run_times.ham_elements = t1 - t0;
+    component_run_times.ham_diag = t2 - t1;
+    double *w = (double *)malloc(sizeof(double) * (size_t)M);
+    if (rc == QD_OK && cudaMemcpy(w, wd, sizeof(double) * (size_t)M, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "copy-out");
+    /* collect_eigenstates.c:23-75 */
+    for (int s = 0; rc == QD_OK && s < M; s++) {
+        struct eigenstate *es = s < 2 * N_states[0] ? &eigenstate_vb[s] : &eigenstate_cb[s - 2 * N_states[0]];
+        es->E = w[s];
+        if (cudaMemcpy(es->fourier, (qd_complex128 *)Zd + (int64_t)s * n, sizeof(qd_complex128) * (size_t)n,
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = qd_set_error(QD_ERR_CUDA, "copy-out");
+    }
+    free(w);
+    cudaFree(Hd);
+    cudaFree(Zd);
+    cudaFree(wd);
+    if (rc) die("eigenstates", rc);
+}
+
+void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coulomb_basis,
+                             struct supercell_geometry *supercell, struct material_params *parameters, int *N_states,
+                             struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb,
+                             struct coulomb_matrix_element CME, int coulomb_region_type);

@@ -1,0 +1,166 @@
+"""ctypes binding of libqdgpu.so (the C-ABI in include/qudos_b200.h).
+
+The library is loaded once, at import.  There is no fallback: if the shared
+library is missing or cannot be loaded the import raises.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqdgpu.so")
+
+QD_OK = 0
+QD_ERR = {1: "INPUT", 2: "UNSUPPORTED", 3: "CUDA", 4: "NOMEM", 5: "CONVERGENCE", 6: "TIMEOUT", 7: "ARG"}
+QD_PREC_FP64, QD_PREC_MIXED = 0, 1
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("libqdgpu.so is not built: run `python qudos_b200/build.py`")
+lib = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
+
+
+class QDError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("qudos_b200 error %d (%s): %s" % (code, QD_ERR.get(code, "?"), msg))
+        self.code = code
+
+
+def check(rc):
+    if rc != QD_OK:
+        raise QDError(rc, lib.qd_last_error_message().decode())
+    return rc
+
+
+class MaterialParams(C.Structure):
+    """struct material_params (8_band.h:200)."""
+    _fields_ = [(n, C.c_double) for n in (
+        "a", "C11", "C12", "C44", "e14", "B114", "B124", "B156", "Eg", "Dso", "Ep", "P", "sc", "g1", "g2", "g3",
+        "ac", "av", "b", "d", "Ev_avg", "E_so", "E_lh", "E_hh", "E_cb", "nr")]
+
+
+class SupercellGeometry(C.Structure):
+    """struct supercell_geometry (8_band.h:197)."""
+    _fields_ = ([(n, C.c_int) for n in ("shape", "embedded", "material", "material_type", "RL1", "RL2", "RL3",
+                                         "RCL1", "RCL2", "RCL3")] +
+                [(n, C.c_double) for n in ("x", "y", "Ox", "Oy", "Oz", "L1", "L2", "L3", "L4", "L5", "SL1", "SL2",
+                                           "SL3", "CL1", "CL2", "CL3", "alpha", "beta", "gamma")])
+
+
+class Vector(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class WaveVectors(C.Structure):
+    """struct wave_vectors (8_band.h:117-124)."""
+    _fields_ = [("N_Gx", C.c_int), ("N_Gy", C.c_int), ("N_Gz", C.c_int), ("N_Gx_T", C.c_int), ("N_Gy_T", C.c_int),
+                ("N_Gz_T", C.c_int), ("Gx", C.POINTER(C.c_double)), ("Gy", C.POINTER(C.c_double)),
+                ("Gz", C.POINTER(C.c_double)), ("Kx", C.c_double), ("Ky", C.c_double), ("Kz", C.c_double)]
+
+
+class Eigenstate(C.Structure):
+    """struct eigenstate (8_band.h:209-211)."""
+    _fields_ = ([("idx_state", C.c_int), ("E", C.c_double)] +
+                [(n, C.POINTER(C.c_double)) for n in ("bloch",) + tuple("probability_%d" % i for i in range(1, 9))] +
+                [(n, C.c_void_p) for n in ("fourier",) + tuple("F_%d" % i for i in range(1, 9))])
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+vp, i64, ci = C.c_void_p, C.c_int64, C.c_int
+_sig("qd_last_error_message", C.c_char_p, [])
+_sig("qd_version", ci, [])
+_sig("qd_problem_load", ci, [C.c_char_p, C.POINTER(C.c_char_p), ci, C.POINTER(vp)])
+_sig("qd_problem_free", None, [vp])
+_sig("qd_problem_sizes", ci, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(ci), C.POINTER(ci), C.POINTER(ci),
+                              C.POINTER(ci)])
+_sig("qd_problem_materials", ci, [vp, C.POINTER(MaterialParams), ci])
+_sig("qd_problem_geometry", ci, [vp, C.POINTER(SupercellGeometry), ci])
+_sig("qd_problem_build_tables", ci, [vp])
+_sig("qd_problem_get_table", ci, [vp, ci, ci, ci, vp, i64])
+_sig("qd_problem_assemble_dev", ci, [vp, vp, i64, ci, ci, vp])
+_sig("qd_eigh_window_dev", ci, [i64, vp, i64, ci, ci, ci, vp, vp, i64, vp])
+_sig("qd_problem_solve", ci, [vp, ci, vp, vp])
+_sig("qd_coulomb", ci, [vp, ci, ci, vp, vp, vp, vp, vp])
+_sig("qd_last_timings", ci, [C.POINTER(C.c_double), ci])
+_sig("qd_dev_alloc", ci, [C.c_size_t, C.POINTER(vp)])
+_sig("qd_dev_free", ci, [vp])
+_sig("qd_memcpy", ci, [vp, vp, C.c_size_t, ci])
+_sig("qd_memset", ci, [vp, ci, C.c_size_t])
+_sig("qd_host_alloc_pinned", ci, [C.c_size_t, C.POINTER(vp)])
+_sig("qd_host_free_pinned", ci, [vp])
+_sig("qd_device_synchronize", ci, [])
+_sig("qd_device_count", ci, [C.POINTER(ci)])
+_sig("qd_set_device", ci, [ci])
+_sig("qd_event_create", ci, [C.POINTER(vp)])
+_sig("qd_event_record", ci, [vp, vp])
+_sig("qd_event_elapsed_ms", ci, [vp, vp, C.POINTER(C.c_float)])
+_sig("qd_event_destroy", ci, [vp])
+_sig("hamiltonian_8_band", None, [ci, Vector, WaveVectors, C.POINTER(SupercellGeometry), C.POINTER(MaterialParams),
+                                  vp])
+_sig("diagonalise_hamiltonian", None, [C.POINTER(ci), vp, vp, vp])
+_sig("eigenstates", None, [ci, C.POINTER(ci), Vector, WaveVectors, C.POINTER(SupercellGeometry),
+                           C.POINTER(MaterialParams), C.POINTER(Eigenstate), C.POINTER(Eigenstate)])
+
+
+def device_count():
+    n = ci(0)
+    rc = lib.qd_device_count(C.byref(n))
+    return n.value if rc == QD_OK else 0
+
+
+class DeviceBuffer:
+    """Owned device allocation."""
+
+    def __init__(self, nbytes):
+        self.ptr = vp()
+        check(lib.qd_dev_alloc(int(nbytes), C.byref(self.ptr)))
+        self.nbytes = int(nbytes)
+
+    def free(self):
+        if self.ptr:
+            lib.qd_dev_free(self.ptr)
+            self.ptr = vp()
+
+    def __del__(self):
+        self.free()
+
+    def upload(self, arr):
+        arr = np.ascontiguousarray(arr)
+        assert arr.nbytes <= self.nbytes
+        check(lib.qd_memcpy(self.ptr, arr.ctypes.data, arr.nbytes, 1))
+
+    def download(self, arr):
+        assert arr.flags.c_contiguous or arr.flags.f_contiguous
+        check(lib.qd_memcpy(arr.ctypes.data, self.ptr, arr.nbytes, 2))
+        return arr
+
+
+class Event:
+    def __init__(self):
+        self.ev = vp()
+        check(lib.qd_event_create(C.byref(self.ev)))
+
+    def record(self, stream=None):
+        check(lib.qd_event_record(self.ev, stream))
+
+    def elapsed_ms(self, later):
+        ms = C.c_float(0)
+        check(lib.qd_event_elapsed_ms(self.ev, later.ev, C.byref(ms)))
+        return float(ms.value)
+
+    def __del__(self):
+        if self.ev:
+            lib.qd_event_destroy(self.ev)
+
+
+def last_timings():
+    a = (C.c_double * 8)()
+    lib.qd_last_timings(a, 8)
+    return list(a)

@@ -1,0 +1,103 @@
+"""Python mirror of the QUDOS PWEM solve path on top of libqdgpu.
+
+`Problem` corresponds to one run of the reference's 8_band_pwem.ex up to and
+including `eigenstates` (code/source/8_band/8_band_main.c:142-763): the same
+`parameters.in` / `supercell.in` files and `-Key=value` overrides, the same
+index window and the same outputs (energies, Bloch characters, envelope
+Fourier coefficients).  Every numerical step runs in libqdgpu on the GPU.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import lib as L
+
+TABLE_CHI, TABLE_STRAIN, TABLE_PHI, TABLE_CONV, TABLE_CHI_S, TABLE_STRAIN_S, TABLE_PHI_S, TABLE_COEF = range(8)
+
+
+class Problem:
+    def __init__(self, directory, overrides=()):
+        self._h = C.c_void_p()
+        arr = (C.c_char_p * max(1, len(overrides)))(*[o.encode() for o in overrides])
+        L.check(L.lib.qd_problem_load(os.fsencode(directory), arr, len(overrides), C.byref(self._h)))
+        n_pw, n_h = C.c_int64(), C.c_int64()
+        lo, hi, nvb, ncb = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        L.check(L.lib.qd_problem_sizes(self._h, C.byref(n_pw), C.byref(n_h), C.byref(lo), C.byref(hi),
+                                       C.byref(nvb), C.byref(ncb)))
+        self.n_pw, self.n_h, self.lo, self.hi = n_pw.value, n_h.value, lo.value, hi.value
+        self.n_vb, self.n_cb = nvb.value, ncb.value
+        self.m = self.hi - self.lo + 1
+
+    def close(self):
+        if self._h:
+            L.lib.qd_problem_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def materials(self, n_shape):
+        arr = (L.MaterialParams * n_shape)()
+        L.check(L.lib.qd_problem_materials(self._h, arr, n_shape))
+        return [{f: getattr(a, f) for f, _ in L.MaterialParams._fields_} for a in arr]
+
+    def geometry(self, n_shape):
+        arr = (L.SupercellGeometry * n_shape)()
+        L.check(L.lib.qd_problem_geometry(self._h, arr, n_shape))
+        return [{f: getattr(a, f) for f, _ in L.SupercellGeometry._fields_} for a in arr]
+
+    def build_tables(self):
+        L.check(L.lib.qd_problem_build_tables(self._h))
+
+    def table(self, which, s, c, shape):
+        out = np.empty(shape, dtype=np.complex128)
+        L.check(L.lib.qd_problem_get_table(self._h, which, s, c, out.ctypes.data, out.size))
+        return out
+
+    def assemble(self, mode=0, prec=L.QD_PREC_FP64):
+        """H on the device, copied back as a numpy array (column-major N_H x N_H)."""
+        n = self.n_h
+        es = 16 if prec == L.QD_PREC_FP64 else 8
+        buf = L.DeviceBuffer(n * n * es)
+        L.check(L.lib.qd_memset(buf.ptr, 0, n * n * es))
+        L.check(L.lib.qd_problem_assemble_dev(self._h, buf.ptr, n, mode, prec, None))
+        L.check(L.lib.qd_device_synchronize())
+        H = np.empty((n, n), dtype=np.complex128 if es == 16 else np.complex64, order="F")
+        buf.download(H)
+        buf.free()
+        return H
+
+    def solve(self, prec=L.QD_PREC_FP64):
+        """Eigenpairs of the window [lo, hi]: (eigval[M], eigvec N_H x M)."""
+        w = np.empty(self.m)
+        v = np.empty((self.n_h, self.m), dtype=np.complex128, order="F")
+        L.check(L.lib.qd_problem_solve(self._h, prec, w.ctypes.data, v.ctypes.data))
+        return w, v
+
+    def energies(self, w, v):
+        """Rows of energies_vb.dat (highest state first) and energies_cb.dat
+        (write_energies.c:23-93; Bloch characters bloch_character.c:23-105)."""
+        m_vb = 2 * self.n_vb
+        a = np.abs(v.reshape(8, self.n_pw, -1, order="F")) ** 2
+        bl = a.sum(axis=1).T
+        rows = np.stack([w, 100.0 * (bl[:, 3] + bl[:, 7]), 100.0 * (bl[:, 2] + bl[:, 6]),
+                         100.0 * (bl[:, 1] + bl[:, 5]), 100.0 * (bl[:, 0] + bl[:, 4])], axis=1)
+        return rows[:m_vb][::-1], rows[m_vb:]
+
+
+def eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream=None):
+    L.check(L.lib.qd_eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream))
+
+
+def write_energies(directory, rows_vb, rows_cb):
+    fmt = "%17.10e\t%17.10e\t%17.10e\t%17.10e\t%17.10e\n"
+    with open(os.path.join(directory, "energies_vb.dat"), "w") as f:
+        f.write("".join(fmt % tuple(r) for r in rows_vb))
+    with open(os.path.join(directory, "energies_cb.dat"), "w") as f:
+        f.write("".join(fmt % tuple(r) for r in rows_cb))

@@ -1,0 +1,59 @@
+"""Small input decks shared by the parity tests (reference file format)."""
+
+import os
+
+from qudos_b200 import configs as C
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def prism(mg, tmp):
+    """The reference's Prism_111 example (rotated hexagonal GaAs prism in AlAs,
+    strain, first + second order piezo) at a reduced plane-wave count."""
+    src = os.path.join(GOLDEN, "prism_111")
+    text = open(os.path.join(src, "parameters.in")).read()
+    lines = []
+    for ln in text.splitlines():
+        k = ln.split(":")[0].strip()
+        if k in ("M_Gx", "M_Gy", "M_Gz", "M_S_Gx", "M_S_Gy", "M_S_Gz", "M_C_Gx", "M_C_Gy", "M_C_Gz"):
+            ln = "%s: %d" % (k, mg)
+        lines.append(ln)
+    d = os.path.join(str(tmp), "prism_%d" % mg)
+    C.write_deck(d, "\n".join(lines) + "\n", open(os.path.join(src, "supercell.in")).read())
+    return d
+
+
+def lens(mg, tmp):
+    return C.write_deck(os.path.join(str(tmp), "lens_%d" % mg), *C.lens_7(mg))
+
+
+def pyramid(mg, tmp):
+    return C.write_deck(os.path.join(str(tmp), "pyr_%d" % mg), *C.pyramid_11(mg, n_states=4))
+
+
+def molecule(mg, tmp):
+    return C.write_deck(os.path.join(str(tmp), "mol_%d" % mg), *C.molecule_15(mg, n_states=4))
+
+
+def nostrain_k(mg, tmp):
+    """No strain; cuboid + pyramid (shape 5) + field along x and a supercell wave vector K."""
+    params = C.parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg, M_S_Gy=mg, M_S_Gz=mg, N_VB=2,
+                               N_CB=2, Strain=0, Piezo=0, Fx=25, Fy=-5, Kx=0.02, Ky=0.01, Kz=-0.015)
+    cell = (C.supercell_record((20.0, 22.0, 18.0)) +
+            C.shape_record(0, 3, 0.3, 0.0, (1.0, -0.5, 0.5), (8.0, 7.0, 4.0)) +
+            C.shape_record(5, 3, 0.0, 0.0, (0.0, 0.0, -2.0), (5.0, 4.0, 3.0)))
+    return C.write_deck(os.path.join(str(tmp), "nsk_%d" % mg), params, cell)
+
+
+def isotropic(mg, tmp):
+    """Isotropic elastic tensor, second-order piezo only, embedded shape."""
+    params = C.parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg, M_S_Gy=mg, M_S_Gz=mg, N_VB=2,
+                               N_CB=2, Isotropic=1, Piezo=3, Fz=-30)
+    cell = (C.supercell_record((24.0, 24.0, 20.0)) +
+            C.shape_record(0, 3, 0.8, 0.0, (0.0, 0.0, 0.0), (12.0, 12.0, 6.0)) +
+            C.shape_record(6, 3, 0.2, 0.0, (0.0, 0.0, -1.5), (5.0, 4.0, 2.0, 3.0), embedded=1))
+    return C.write_deck(os.path.join(str(tmp), "iso_%d" % mg), params, cell)
+
+
+CASES = {"prism": prism, "lens": lens, "pyramid": pyramid, "molecule": molecule, "nostrain_k": nostrain_k,
+         "isotropic": isotropic}

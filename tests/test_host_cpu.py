@@ -1,0 +1,103 @@
+"""Host-side logic of libqdgpu on the CPU: input readers, material
+interpolation, error reporting and the exported C-ABI.  No GPU needed."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import qudos_b200 as q
+from qudos_b200 import lib as L
+from oracle import inputs, materials
+import cases
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "qudos_b200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    names = set(re.findall(r"\b(qd_[a-z0-9_]+)\s*\(", hdr))
+    names |= {"hamiltonian_8_band", "diagonalise_hamiltonian", "eigenstates", "coulomb_matrix_elements"}
+    missing = [n for n in sorted(names) if not hasattr(L.lib, n)]
+    assert not missing, missing
+    for g in ("N_H", "na_rows", "characteristic_function_G", "strain_G", "convolutions_char_strain",
+              "phi_piezo_G", "include_strain", "include_piezo", "component_run_times"):
+        ctypes.c_int.in_dll(L.lib, g)  # global exported
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_inputs_and_materials_match_oracle(name, tmp_path):
+    d = cases.CASES[name](2, tmp_path)
+    pr = q.Problem(d)
+    p, geo = inputs.load(d)
+    ns = p["N_shape"]
+    om = materials.material_parameters(p["T"], inputs.clone(geo), p["Piezo"])
+    cm = pr.materials(ns)
+    for s in range(ns):
+        for k in om[s]:
+            assert cm[s][k] == pytest.approx(om[s][k], rel=0, abs=1e-15), (s, k)
+    cg = pr.geometry(ns)
+    for s in range(ns):
+        for k in ("shape", "embedded", "material", "x", "y", "Ox", "Oy", "Oz", "L1", "L2", "L3", "L4", "SL1", "SL2",
+                  "SL3", "CL1", "alpha", "beta", "gamma"):
+            assert cg[s][k] == geo[s][k], (s, k)
+    n_pw = p["N_Gx"] * p["N_Gy"] * p["N_Gz"]
+    assert pr.n_pw == n_pw and pr.n_h == 8 * n_pw
+    assert (pr.lo, pr.hi) == (6 * n_pw - 2 * p["N_VB"], 6 * n_pw + 2 * p["N_CB"] - 1)
+
+
+def test_golden_inputs_parse(tmp_path):
+    pr = q.Problem(os.path.join(ROOT, "tests", "golden", "prism_111"))
+    assert pr.n_h == 10648 and (pr.lo, pr.hi) == (7978, 7989)
+    pr2 = q.Problem(os.path.join(ROOT, "tests", "golden", "prism_111"), ["-M_Gx=2", "-N_VB=2"])
+    assert pr2.n_pw == 5 * 11 * 11 and pr2.hi - pr2.lo + 1 == 2 * 2 + 2 * 2
+
+
+def _write(tmp_path, params, cell):
+    (tmp_path / "parameters.in").write_text(params)
+    (tmp_path / "supercell.in").write_text(cell)
+    return str(tmp_path)
+
+
+def test_missing_parameter_is_an_error_not_an_exit(tmp_path):
+    from qudos_b200 import configs as C
+    params = C.parameters_text().replace("Piezo: 1\n", "")
+    d = _write(tmp_path, params, C.lens_7()[1])
+    with pytest.raises(q.QDError) as e:
+        q.Problem(d)
+    assert e.value.code == 1 and "Piezo" in str(e.value)
+
+
+def test_shape_count_mismatch(tmp_path):
+    from qudos_b200 import configs as C
+    p, c = C.lens_7()
+    d = _write(tmp_path, p.replace("N_shape: 3", "N_shape: 4"), c)
+    with pytest.raises(q.QDError, match="greater than the number of shapes"):
+        q.Problem(d)
+    d2 = _write(tmp_path, p.replace("N_shape: 3", "N_shape: 2"), c)
+    with pytest.raises(q.QDError, match="less than the number of shapes"):
+        q.Problem(d2)
+
+
+def test_unknown_material_and_missing_file(tmp_path):
+    from qudos_b200 import configs as C
+    p, c = C.lens_7()
+    d = _write(tmp_path, p, c.replace("Material: 3", "Material: 22", 1))
+    with pytest.raises(q.QDError, match="material system"):
+        q.Problem(d)
+    with pytest.raises(q.QDError, match="parameters.in"):
+        q.Problem(str(tmp_path / "nowhere"))
+
+
+def test_malformed_line_and_override(tmp_path):
+    from qudos_b200 import configs as C
+    p, c = C.lens_7()
+    d = _write(tmp_path, p + "this line has no colon\n", c)
+    with pytest.raises(q.QDError, match="malformed"):
+        q.Problem(d)
+    d = _write(tmp_path, p, c)
+    with pytest.raises(q.QDError, match="override"):
+        q.Problem(d, ["M_Gx=3"])
