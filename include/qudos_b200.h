@@ -162,6 +162,10 @@ typedef struct qd_problem qd_problem;
  * and material parameters on the host. */
 int qd_problem_load(const char *dir, const char *const *overrides, int n_overrides, qd_problem **out);
 void qd_problem_free(qd_problem *pr);
+int qd_problem_n_shape(const qd_problem *pr);
+/* Number of libqdgpu kernel launches since the library was loaded (library
+ * GEMMs from cuBLAS not included). */
+long long qd_launch_count(void);
 /* Sizes: n_pw = N_Gx N_Gy N_Gz, n_h = 8 n_pw, window [lo, hi] 0-based. */
 int qd_problem_sizes(const qd_problem *pr, int64_t *n_pw, int64_t *n_h, int *lo, int *hi,
                      int *n_vb, int *n_cb);

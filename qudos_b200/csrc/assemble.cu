@@ -186,6 +186,7 @@ extern "C" int qd_assemble_launch(const void *d_coef, const double *d_Gx, const 
     dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
     cudaStream_t st = (cudaStream_t)stream;
     int full = mode == 1;
+    qd_count_launch(1);
     if (prec == QD_PREC_FP64)
         assemble_kernel<1><<<grid, 128, 0, st>>>(c, npw, nh, (double2 *)H, nullptr, ld, full, cols_per);
     else if (prec == QD_PREC_MIXED)
@@ -215,6 +216,7 @@ extern "C" int qd_assemble_dual_launch(const void *d_coef, const double *d_Gx, c
     int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
     const int cols_per = 16;
     dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
+    qd_count_launch(1);
     assemble_kernel<3><<<grid, 128, 0, (cudaStream_t)stream>>>(c, npw, nh, (double2 *)H64, (float2 *)H32, ld,
                                                                 mode == 1, cols_per);
     cudaError_t e = cudaGetLastError();

@@ -9,6 +9,16 @@ struct cpx {
     R re, im;
 };
 
+// Workspace of the dense -> band reduction (eig_stage1.cu).
+struct Stage1Work {
+    void *VT, *X, *M, *Y, *Tall, *Rall, *Vacc, *Wacc, *S1, *S2, *gram, *tau;
+    double2 *red, *rowbuf;
+    unsigned *bar;
+    int *err;
+    int npanels, agg;
+    int64_t ldv;
+};
+
 template <typename R>
 __device__ __forceinline__ cpx<R> mk(R a, R b) {
     cpx<R> z;

@@ -23,13 +23,6 @@
 
 typedef cpx<double> zd;
 
-struct Stage1Work {
-    void *VT, *X, *M, *Y, *Tall, *Rall;
-    double *red;
-    unsigned *bar;
-    int *err;
-    int npanels;
-};
 extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w);
 extern "C" void qd_stage1_free(Stage1Work *w);
 extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, Stage1Work *w, void *stream);
@@ -342,6 +335,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     float2 *H32 = nullptr;
     if (mixed) {
         CUDA_OK(cudaMalloc(&H32, sizeof(float2) * n * n));
+        qd_count_launch(1);
         lower64_to_full32_kernel<<<dim3((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)n), 256, 0, st>>>(
             (const double2 *)H, ld, n, H32, n);
         CUDA_OK(cudaGetLastError());
@@ -378,6 +372,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     unsigned long long *dmax;
     CUDA_OK(cudaMalloc(&dmax, sizeof(unsigned long long)));
     CUDA_OK(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st));
+    qd_count_launch(1);
     band_absmax_kernel<<<64, 256, 0, st>>>(AB0, ldb, n, b, dmax);
     unsigned long long bm_bits = 0;
     CUDA_OK(cudaMemcpyAsync(&bm_bits, dmax, sizeof(bm_bits), cudaMemcpyDeviceToHost, st));
@@ -418,6 +413,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     } else {
         float2 *Z32;
         CUDA_OK(cudaMalloc(&Z32, sizeof(float2) * n * k));
+        qd_count_launch(4);
         c128_to_c64_kernel<<<dim3(64, k), 256, 0, st>>>(Zb, n, Z32, n, n);
         RC(qd_stage1_backtransform(A, n, lda, b, 1, &w1, Z32, n, k, st));
         c64_to_c128_kernel<<<dim3(64, k), 256, 0, st>>>(Z32, n, Zb, n, n);

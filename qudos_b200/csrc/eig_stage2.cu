@@ -27,6 +27,7 @@ typedef cpx<double> zd;
 
 #define SPIN_LIMIT (1LL << 25)
 #define PROGRESS_DONE 0x7fffffff
+#define QD_INVIT_ITERS 2
 
 // ---------------------------------------------------------------------------
 // Householder helpers in shared memory (one warp computes, results broadcast)
@@ -95,72 +96,121 @@ __device__ __forceinline__ void stab(double2 *AB, int ldb, int64_t i, int64_t j,
     __stcg(&AB[(i - j) + j * (int64_t)ldb], make_double2(v.re, v.im));
 }
 
-__device__ bool wait_progress(volatile int *progress, int s_prev, int need, int *err) {
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ bool wait_progress(const int *progress, int s_prev, int need, int *err) {
     __shared__ int ok;
     if (threadIdx.x == 0) {
         ok = 1;
         long long it = 0;
-        while (true) {
-            int p = progress[s_prev];
-            if (p >= need) break;
+        while (ld_acquire(progress + s_prev) < need) {
             if (++it > SPIN_LIMIT || *(volatile int *)err) {
                 atomicExch(err, QD_ERR_TIMEOUT);
                 ok = 0;
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(20);
         }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
 }
 
-__device__ void publish(int *progress, int s, int val) {
+__device__ __forceinline__ void publish(int *progress, int s, int val) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicExch(&progress[s], val);
+        st_release(progress + s, val);
     }
 }
 
-__global__ void __launch_bounds__(128) hb2st_kernel(double2 *AB, int ldb, int n, int b, int *progress, int *err) {
+// 8 threads per output: out[o] = sum_i M(o, i) * x[i] (complex), n_out <= 32, n_in <= 32.
+// mode 0: out[r] = sum_c E[r + c*ld] x[c]; mode 1: out[c] = sum_r conj(x[r]) E[r + c*ld].
+// Every lane of the warp must call it (the reduction shuffles over all 32 lanes);
+// lanes whose output index is out of range pass valid = false.
+__device__ __forceinline__ zd dot8(const zd *E, int ld, const zd *x, int o, int n_in, int part, int mode, bool valid) {
+    zd acc = mk<double>(0, 0);
+    for (int i = part; valid && i < n_in; i += 8) {
+        if (mode == 0) acc = cadd(acc, cmul(E[o + i * ld], x[i]));
+        else acc = cadd(acc, cmulc(x[i], E[i + o * ld]));
+    }
+    for (int off = 4; off > 0; off >>= 1) {
+        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, off);
+        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, off);
+    }
+    return acc;
+}
+
+// c = Re(conj(tau) v^H u) for vectors of length n <= 32, computed by a whole warp.
+__device__ __forceinline__ double warp_vhu(const zd *v, const zd *u, zd tau, int n) {
+    int lane = threadIdx.x & 31;
+    double part = 0.0;
+    if (lane < n) part = cmulc(tau, cmulc(v[lane], u[lane])).re;
+    return warp_sum(part);
+}
+
+// Two-sided update of the Hermitian block D (n x n, ld b) with H = I - tau v v^H,
+// given u = tau D v: D <- D - v u'^H - u' v^H, u' = u - 1/2 c v, c = Re(conj(tau) v^H u).
+// Writes the lower triangle to the band at (r0, r0).
+__device__ __forceinline__ void sym_apply_store(zd *D, int ldD, int n, const zd *v, const zd *u, zd tau, double2 *AB,
+                                                int ldb, int64_t r0) {
+    double c = warp_vhu(v, u, tau, n);
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        int r = idx % n, q = idx / n;
+        if (r < q) continue;
+        zd ur = csub(u[r], mk<double>(0.5 * c * v[r].re, 0.5 * c * v[r].im));
+        zd uq = csub(u[q], mk<double>(0.5 * c * v[q].re, 0.5 * c * v[q].im));
+        zd val = csub(D[r + q * ldD], cadd(cmul(v[r], cconj(uq)), cmul(ur, cconj(v[q]))));
+        if (r == q) val.im = 0.0;
+        stab(AB, ldb, r0 + r, r0 + q, val);
+    }
+}
+
+__global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n, int b, int *progress, int *err) {
     extern __shared__ unsigned char sm_raw[];
     zd *D = (zd *)sm_raw;        // b x b
     zd *E = D + b * b;           // b x b
-    zd *v = E + b * b;           // b
-    zd *v2 = v + b;              // b
-    zd *w = v2 + b;              // b
-    __shared__ double scratch[33];
+    zd *va = E + b * b;          // b : current reflector
+    zd *vb = va + b;             // b : next reflector
+    zd *u = vb + b;              // b
+    zd *w = u + b;               // b
     __shared__ double s_beta;
     __shared__ zd s_tau;
+    const int t = threadIdx.x, part = t & 7, o8 = t >> 3;
     for (int s = blockIdx.x; s < n - 1; s += gridDim.x) {
+        zd *v = va, *v2 = vb;
         // ---- task 0: annihilate column s below the subdiagonal
         if (s > 0 && !wait_progress(progress, s - 1, 3, err)) return;
         int st = s + 1, ed = min(s + b, n - 1), len = ed - st + 1;
-        for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = ldab(AB, ldb, st + i, s);
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            double beta;
-            zd tau;
-            larfg_warp(v, len, &beta, &tau);
-            if (threadIdx.x == 0) { s_beta = beta; s_tau = tau; }
-        }
-        __syncthreads();
-        zd tau = s_tau;
-        for (int i = threadIdx.x; i < len; i += blockDim.x)
-            stab(AB, ldb, st + i, s, i == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0));
-        // diagonal block [st, ed]
-        for (int idx = threadIdx.x; idx < len * len; idx += blockDim.x) {
+        for (int i = t; i < len; i += blockDim.x) v[i] = ldab(AB, ldb, st + i, s);
+        for (int idx = t; idx < len * len; idx += blockDim.x) {
             int r = idx % len, c = idx / len;
             D[r + c * b] = r >= c ? ldab(AB, ldb, st + r, st + c) : cconj(ldab(AB, ldb, st + c, st + r));
         }
         __syncthreads();
-        sym_update(D, b, len, v, tau, w, scratch);
-        for (int idx = threadIdx.x; idx < len * len; idx += blockDim.x) {
-            int r = idx % len, c = idx / len;
-            if (r >= c) stab(AB, ldb, st + r, st + c, D[r + c * b]);
+        if (t < 32) {
+            double beta;
+            zd tau;
+            larfg_warp(v, len, &beta, &tau);
+            if (t == 0) { s_beta = beta; s_tau = tau; }
         }
+        __syncthreads();
+        zd tau = s_tau;
+        for (int i = t; i < len; i += blockDim.x)
+            stab(AB, ldb, st + i, s, i == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0));
+        {
+            zd acc = dot8(D, b, v, o8, len, part, 0, o8 < len);
+            if (part == 0 && o8 < len) u[o8] = cmul(tau, acc);
+        }
+        __syncthreads();
+        sym_apply_store(D, b, len, v, u, tau, AB, ldb, st);
         publish(progress, s, 1);
         int k = 1;
         while (true) {
@@ -168,43 +218,47 @@ __global__ void __launch_bounds__(128) hb2st_kernel(double2 *AB, int ldb, int n,
             if (J1 > n - 1) break;
             int J2 = min(ed + b, n - 1), lm = J2 - J1 + 1;
             if (s > 0 && !wait_progress(progress, s - 1, k + 3, err)) return;
-            // E = A[J1..J2, st..ed]
-            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+            // E = A[J1..J2, st..ed] and D = A[J1..J2, J1..J2] in one round trip
+            for (int idx = t; idx < lm * len; idx += blockDim.x) {
                 int r = idx % lm, c = idx / lm;
                 E[r + c * b] = ldab(AB, ldb, J1 + r, st + c);
             }
-            __syncthreads();
-            // right application of the previous reflector: E <- E - tau (E v) v^H
-            for (int r = threadIdx.x; r < lm; r += blockDim.x) {
-                zd acc = mk<double>(0, 0);
-                for (int c = 0; c < len; c++) acc = cadd(acc, cmul(E[r + c * b], v[c]));
-                w[r] = cmul(tau, acc);
+            for (int idx = t; idx < lm * lm; idx += blockDim.x) {
+                int r = idx % lm, c = idx / lm;
+                D[r + c * b] = r >= c ? ldab(AB, ldb, J1 + r, J1 + c) : cconj(ldab(AB, ldb, J1 + c, J1 + r));
             }
             __syncthreads();
-            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+            // right application of the previous reflector: E <- E - tau (E v) v^H
+            {
+                zd acc = dot8(E, b, v, o8, len, part, 0, o8 < lm);
+                if (part == 0 && o8 < lm) w[o8] = cmul(tau, acc);
+            }
+            __syncthreads();
+            for (int idx = t; idx < lm * len; idx += blockDim.x) {
                 int r = idx % lm, c = idx / lm;
                 E[r + c * b] = csub(E[r + c * b], cmul(w[r], cconj(v[c])));
             }
             __syncthreads();
             // new reflector from E[:, 0]
-            for (int i = threadIdx.x; i < lm; i += blockDim.x) v2[i] = E[i];
-            __syncthreads();
-            if (threadIdx.x < 32) {
+            if (t < 32) {
+                for (int i = t; i < lm; i += 32) v2[i] = E[i];
+                __syncwarp();
                 double beta;
                 zd t2;
                 larfg_warp(v2, lm, &beta, &t2);
-                if (threadIdx.x == 0) { s_beta = beta; s_tau = t2; }
+                if (t == 0) { s_beta = beta; s_tau = t2; }
             }
             __syncthreads();
             zd tau2 = s_tau;
-            // left application to the remaining columns: E <- E - conj(tau2) v2 (v2^H E)
-            for (int c = 1 + threadIdx.x; c < len; c += blockDim.x) {
-                zd acc = mk<double>(0, 0);
-                for (int r = 0; r < lm; r++) acc = cadd(acc, cmulc(v2[r], E[r + c * b]));
-                w[c] = cmul(cconj(tau2), acc);
+            // left application coefficients and u = tau2 D v2 in the same phase
+            {
+                zd acc = dot8(E, b, v2, o8, lm, part, 1, o8 > 0 && o8 < len);
+                if (part == 0 && o8 > 0 && o8 < len) w[o8] = cmul(cconj(tau2), acc);
+                zd acc2 = dot8(D, b, v2, o8, lm, part, 0, o8 < lm);
+                if (part == 0 && o8 < lm) u[o8] = cmul(tau2, acc2);
             }
             __syncthreads();
-            for (int idx = threadIdx.x; idx < lm * len; idx += blockDim.x) {
+            for (int idx = t; idx < lm * len; idx += blockDim.x) {
                 int r = idx % lm, c = idx / lm;
                 zd val;
                 if (c == 0) val = r == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0);
@@ -212,18 +266,10 @@ __global__ void __launch_bounds__(128) hb2st_kernel(double2 *AB, int ldb, int n,
                 stab(AB, ldb, J1 + r, st + c, val);
             }
             __syncthreads();
-            // diagonal block [J1, J2]
-            for (int idx = threadIdx.x; idx < lm * lm; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                D[r + c * b] = r >= c ? ldab(AB, ldb, J1 + r, J1 + c) : cconj(ldab(AB, ldb, J1 + c, J1 + r));
-            }
-            __syncthreads();
-            sym_update(D, b, lm, v2, tau2, w, scratch);
-            for (int idx = threadIdx.x; idx < lm * lm; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                if (r >= c) stab(AB, ldb, J1 + r, J1 + c, D[r + c * b]);
-            }
-            for (int i = threadIdx.x; i < lm; i += blockDim.x) v[i] = v2[i];
+            sym_apply_store(D, b, lm, v2, u, tau2, AB, ldb, J1);
+            zd *tmp = v;
+            v = v2;
+            v2 = tmp;
             tau = tau2;
             st = J1;
             ed = J2;
@@ -431,7 +477,7 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
     zd *fb = lcol + b + warp * 192;  // 64 slots forward window
     zd *bb = fb + 64;                // 128 slots backward window
-    for (int it = 0; it < 3; it++) {
+    for (int it = 0; it < QD_INVIT_ITERS; it++) {
         for (int q = warp; q < gs; q += nwarp) {
             double2 *y = ywork + ((int64_t)blockIdx.x * 8 + warp) * n;
             double2 *x = Z + (int64_t)(m0 + q) * ldz;
@@ -447,9 +493,16 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
             };
             for (int i = lane; i <= b && i < n; i += 32) fb[i & 63] = rhs(i);
             __syncwarp();
-            // forward: P and L
+            // forward: P and L (the next step's pivot and multipliers are fetched ahead)
+            int p_next = ipiv[0];
+            double2 l_next = lane < b ? L[lane] : make_double2(0.0, 0.0);
             for (int j = 0; j < n; j++) {
-                int p = ipiv[j];
+                int p = p_next;
+                double2 l = l_next;
+                if (j + 1 < n) {
+                    p_next = ipiv[j + 1];
+                    if (lane < b) l_next = L[(int64_t)(j + 1) * b + lane];
+                }
                 if (lane == 0 && p != j) {
                     zd t = fb[j & 63];
                     fb[j & 63] = fb[p & 63];
@@ -458,32 +511,36 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
                 __syncwarp();
                 zd yj = fb[j & 63];
                 int i = j + 1 + lane;
-                if (lane < b && i < n) {
-                    double2 l = L[(int64_t)j * b + lane];
-                    fb[i & 63] = csub(fb[i & 63], cmul(mk<double>(l.x, l.y), yj));
-                }
+                if (lane < b && i < n) fb[i & 63] = csub(fb[i & 63], cmul(mk<double>(l.x, l.y), yj));
                 if (lane == 0) y[j] = make_double2(yj.re, yj.im);
                 if (lane == 1 && j + b + 1 < n) fb[(j + b + 1) & 63] = rhs(j + b + 1);
                 __syncwarp();
             }
-            // backward: U x = y
+            // backward: U x = y (row j of U fetched one step ahead)
+            auto urow = [&](int j, double2 &u0, double2 &u1, double2 &ud, double2 &yy) {
+                int c0 = j + 1 + lane, c1 = j + 33 + lane, cend = min(j + 2 * b, n - 1);
+                u0 = c0 <= cend ? U[(int64_t)j * cols + (c0 - j)] : make_double2(0.0, 0.0);
+                u1 = c1 <= cend ? U[(int64_t)j * cols + (c1 - j)] : make_double2(0.0, 0.0);
+                ud = U[(int64_t)j * cols];
+                yy = y[j];
+            };
+            double2 nu0, nu1, nud, nyy;
+            urow(n - 1, nu0, nu1, nud, nyy);
             for (int j = n - 1; j >= 0; j--) {
-                double sr = 0.0, si = 0.0;
+                double2 u0 = nu0, u1 = nu1, ud = nud, yy = nyy;
+                if (j > 0) urow(j - 1, nu0, nu1, nud, nyy);
+                int c0 = j + 1 + lane, c1 = j + 33 + lane;
                 int cend = min(j + 2 * b, n - 1);
-                for (int c = j + 1 + lane; c <= cend; c += 32) {
-                    double2 u = U[(int64_t)j * cols + (c - j)];
-                    zd xc = bb[c & 127];
-                    sr += u.x * xc.re - u.y * xc.im;
-                    si += u.x * xc.im + u.y * xc.re;
-                }
+                zd x0 = c0 <= cend ? bb[c0 & 127] : mk<double>(0, 0);
+                zd x1 = c1 <= cend ? bb[c1 & 127] : mk<double>(0, 0);
+                double sr = u0.x * x0.re - u0.y * x0.im + u1.x * x1.re - u1.y * x1.im;
+                double si = u0.x * x0.im + u0.y * x0.re + u1.x * x1.im + u1.y * x1.re;
                 sr = warp_sum(sr);
                 si = warp_sum(si);
                 if (lane == 0) {
-                    double2 u = U[(int64_t)j * cols];
-                    double2 yy = y[j];
                     double rr = yy.x - sr, ri = yy.y - si;
-                    double den = u.x * u.x + u.y * u.y;
-                    zd xj = mk<double>((rr * u.x + ri * u.y) / den, (ri * u.x - rr * u.y) / den);
+                    double den = ud.x * ud.x + ud.y * ud.y;
+                    zd xj = mk<double>((rr * ud.x + ri * ud.y) / den, (ri * ud.x - rr * ud.y) / den);
                     bb[j & 127] = xj;
                     x[j] = make_double2(xj.re, xj.im);
                 }
@@ -534,12 +591,12 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
 
 extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *err, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    size_t smem = (size_t)(2 * b * b + 3 * b) * sizeof(zd);
+    size_t smem = (size_t)(2 * b * b + 4 * b) * sizeof(zd);
     CUDA_OK(cudaFuncSetAttribute(hb2st_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev, nsm, per_sm = 0;
     CUDA_OK(cudaGetDevice(&dev));
     CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 128, smem));
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 256, smem));
     if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
     int G = nsm * per_sm;
     int useful = n / (2 * b) + 2;  // concurrent sweeps are limited by the 3-task lag
@@ -549,13 +606,15 @@ extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *
     CUDA_OK(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n, st));
     CUDA_OK(cudaMemsetAsync(err, 0, sizeof(int), st));
     void *args[] = {&AB, &ldb, &n, &b, &progress, &err};
-    CUDA_OK(cudaLaunchCooperativeKernel((void *)hb2st_kernel, dim3(G), dim3(128), args, smem, st));
+    qd_count_launch(1);
+    CUDA_OK(cudaLaunchCooperativeKernel((void *)hb2st_kernel, dim3(G), dim3(256), args, smem, st));
     return QD_OK;
 }
 
 extern "C" int qd_tridiag_bisect(const double2 *AB, int ldb, int n, int lo, int hi, double *d, double *e2,
                                  double *bounds, double *w, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
+    qd_count_launch(3);
     tri_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(AB, ldb, n, d, e2);
     gersh_kernel<<<1, 1024, 0, st>>>(d, e2, n, bounds);
     int m = hi - lo + 1;
@@ -570,6 +629,7 @@ extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const do
     cudaStream_t st = (cudaStream_t)stream;
     size_t smem = (size_t)((b + 1) * (2 * b + 1) + b + 8 * 192) * sizeof(zd);
     CUDA_OK(cudaFuncSetAttribute(band_invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    qd_count_launch(1);
     band_invit_kernel<<<ngroups, 256, smem, st>>>(AB0, ldb, n, b, lam_dev, gstart_dev, gsize_dev, Lw, Uw, ipivw, Z,
                                                   ldz, bnorm, ywork);
     CUDA_OK(cudaGetLastError());

@@ -55,6 +55,12 @@ int qd_set_error(int code, const char *fmt, ...) {
 const char *qd_last_error_message(void) { return g_err; }
 int qd_version(void) { return 1; }
 
+/* Number of this library's own kernel launches since load (cuBLAS calls not
+ * included); read by callers that report how much of a step ran in our kernels. */
+static long long g_launches = 0;
+void qd_count_launch(int n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
+long long qd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
 /* Device-memory, copy and event helpers so that callers without a CUDA
  * toolkit binding (ctypes, Fortran, ...) can drive the device-resident entry
  * points. */
@@ -269,6 +275,8 @@ void qd_problem_free(qd_problem *pr) {
     free(pr->mat);
     free(pr);
 }
+
+int qd_problem_n_shape(const qd_problem *pr) { return pr ? pr->p.n_shape : 0; }
 
 int qd_problem_sizes(const qd_problem *pr, int64_t *n_pw, int64_t *n_h, int *lo, int *hi, int *n_vb, int *n_cb) {
     if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");

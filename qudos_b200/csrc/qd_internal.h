@@ -53,6 +53,8 @@ int qd_material_parameters(double T, int include_piezo, int n_shape, struct supe
                            struct material_params *out);
 void qd_basis_grid(int n_T, double L, double *out);
 
+void qd_count_launch(int n);
+
 /* error state (api.cu) */
 int qd_set_error(int code, const char *fmt, ...);
 

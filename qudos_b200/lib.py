@@ -78,6 +78,8 @@ _sig("qd_last_error_message", C.c_char_p, [])
 _sig("qd_version", ci, [])
 _sig("qd_problem_load", ci, [C.c_char_p, C.POINTER(C.c_char_p), ci, C.POINTER(vp)])
 _sig("qd_problem_free", None, [vp])
+_sig("qd_problem_n_shape", ci, [vp])
+_sig("qd_launch_count", C.c_longlong, [])
 _sig("qd_problem_sizes", ci, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(ci), C.POINTER(ci), C.POINTER(ci),
                               C.POINTER(ci)])
 _sig("qd_problem_materials", ci, [vp, C.POINTER(MaterialParams), ci])

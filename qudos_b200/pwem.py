@@ -29,6 +29,7 @@ class Problem:
         self.n_pw, self.n_h, self.lo, self.hi = n_pw.value, n_h.value, lo.value, hi.value
         self.n_vb, self.n_cb = nvb.value, ncb.value
         self.m = self.hi - self.lo + 1
+        self.n_shape = L.lib.qd_problem_n_shape(self._h)
 
     def close(self):
         if self._h:
@@ -84,7 +85,7 @@ class Problem:
         """Rows of energies_vb.dat (highest state first) and energies_cb.dat
         (write_energies.c:23-93; Bloch characters bloch_character.c:23-105)."""
         m_vb = 2 * self.n_vb
-        a = np.abs(v.reshape(8, self.n_pw, -1, order="F")) ** 2
+        a = np.abs(v.reshape(8, self.n_pw, -1)) ** 2  # row = band * n_pw + plane wave
         bl = a.sum(axis=1).T
         rows = np.stack([w, 100.0 * (bl[:, 3] + bl[:, 7]), 100.0 * (bl[:, 2] + bl[:, 6]),
                          100.0 * (bl[:, 1] + bl[:, 5]), 100.0 * (bl[:, 0] + bl[:, 4])], axis=1)

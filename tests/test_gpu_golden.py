@@ -25,5 +25,8 @@ def test_prism_111_golden(prec):
     gcb = np.loadtxt(os.path.join(GOLDEN, "energies_cb.dat"))
     assert np.abs(vb[:, 0] - gvb[:, 0]).max() < 5e-9
     assert np.abs(cb[:, 0] - gcb[:, 0]).max() < 5e-9
-    assert np.abs(_kramers(vb) - _kramers(gvb)).max() < 1e-6
-    assert np.abs(_kramers(cb) - _kramers(gcb)).max() < 1e-6
+    # Bloch characters in percent; the mixed path's vectors carry FP32-level
+    # subspace errors before refinement, so its tolerance is looser
+    tol = 1e-6 if prec == q.QD_PREC_FP64 else 1e-3
+    assert np.abs(_kramers(vb) - _kramers(gvb)).max() < tol
+    assert np.abs(_kramers(cb) - _kramers(gcb)).max() < tol
