@@ -229,6 +229,23 @@ int qd_event_destroy(void *ev);
  * [4] inverse iteration, [5] back-transform, [6] refinement. */
 int qd_last_timings(double *ms, int n);
 
+/* Allocation-free eigenvalues of a Hermitian tridiagonal matrix for the index
+ * window [lo, hi] (0-based, ascending), by the same Sturm-count multisection
+ * as the solver's bisection stage.  No reference counterpart: it serves
+ * callers that may not allocate device memory (code running inside a stream
+ * capture, or under a caller-owned memory budget).
+ *   AB: device, band storage with ldb >= 2; AB[j*ldb] is the diagonal entry
+ *       (real part used), AB[1 + j*ldb] the sub-diagonal entry (j, j+1).
+ *   w:  device, hi - lo + 1 doubles.
+ * Scratch is file-scope device memory for n <= QD_STATIC_TRI_MAX rows; larger
+ * n returns QD_ERR_ARG.  The scratch is shared by all calls on a device, so
+ * calls that may overlap (several streams or host threads) must be
+ * serialised by the caller.  The first call on each device resolves the
+ * scratch addresses (cudaGetSymbolAddress); make that first call outside any
+ * stream capture. */
+#define QD_STATIC_TRI_MAX 65536
+int qd_tridiag_eigvals_noalloc(const void *AB, int ldb, int n, int lo, int hi, double *w, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

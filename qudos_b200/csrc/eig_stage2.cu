@@ -635,3 +635,52 @@ extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const do
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of qd_tridiag_bisect for callers that may not
+// allocate device memory (see the declaration in qudos_b200.h).  The
+// per-call scratch (diagonal, squared off-diagonal, Gershgorin bounds) lives
+// in file-scope device arrays sized for QD_STATIC_TRI_MAX rows; the kernels
+// and their launch shapes are those of qd_tridiag_bisect.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_static_tri_d[QD_STATIC_TRI_MAX];
+static __device__ __align__(256) double g_static_tri_e2[QD_STATIC_TRI_MAX];
+static __device__ __align__(256) double g_static_tri_bounds[4];
+
+#define QD_STATIC_MAX_DEVICES 64
+static double *g_static_addr[QD_STATIC_MAX_DEVICES][3];
+
+extern "C" int qd_tridiag_eigvals_noalloc(const void *ABv, int ldb, int n, int lo, int hi, double *w,
+                                          void *stream) {
+    const double2 *AB = (const double2 *)ABv;
+    if (n < 1 || n > QD_STATIC_TRI_MAX)
+        return qd_set_error(QD_ERR_ARG, "qd_tridiag_eigvals_noalloc: n = %d outside [1, %d]", n, QD_STATIC_TRI_MAX);
+    if (ldb < 2 || lo < 0 || hi < lo || hi >= n || !AB || !w)
+        return qd_set_error(QD_ERR_ARG, "qd_tridiag_eigvals_noalloc: bad arguments (ldb %d, window [%d, %d])", ldb,
+                            lo, hi);
+    int dev = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= QD_STATIC_MAX_DEVICES)
+        return qd_set_error(QD_ERR_ARG, "qd_tridiag_eigvals_noalloc: device %d not supported", dev);
+    double **a = g_static_addr[dev];
+    if (!a[0]) {  // first call on this device: resolve the scratch addresses once
+        void *p0 = nullptr, *p1 = nullptr, *p2 = nullptr;
+        CUDA_OK(cudaGetSymbolAddress(&p0, g_static_tri_d));
+        CUDA_OK(cudaGetSymbolAddress(&p1, g_static_tri_e2));
+        CUDA_OK(cudaGetSymbolAddress(&p2, g_static_tri_bounds));
+        a[1] = (double *)p1;
+        a[2] = (double *)p2;
+        a[0] = (double *)p0;
+    }
+    // Every scratch element that is read is written first in the same call
+    // (d and e2 for the n rows by tri_extract_kernel, the bounds by
+    // gersh_kernel), so nothing needs clearing.
+    cudaStream_t st = (cudaStream_t)stream;
+    qd_count_launch(3);
+    tri_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(AB, ldb, n, a[0], a[1]);
+    gersh_kernel<<<1, 1024, 0, st>>>(a[0], a[1], n, a[2]);
+    int m = hi - lo + 1;
+    bisect_kernel<<<(m * 32 + 127) / 128, 128, 0, st>>>(a[0], a[1], n, lo, hi, a[2], w);
+    CUDA_OK(cudaGetLastError());
+    return QD_OK;
+}

@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(HERE, "libqdgpu.so")
 QD_OK = 0
 QD_ERR = {1: "INPUT", 2: "UNSUPPORTED", 3: "CUDA", 4: "NOMEM", 5: "CONVERGENCE", 6: "TIMEOUT", 7: "ARG"}
 QD_PREC_FP64, QD_PREC_MIXED = 0, 1
+QD_ERR_ARG = 7
+QD_STATIC_TRI_MAX = 65536  # rows of the allocation-free tridiagonal scratch
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("libqdgpu.so is not built: run `python qudos_b200/build.py`")
@@ -91,6 +93,8 @@ _sig("qd_eigh_window_dev", ci, [i64, vp, i64, ci, ci, ci, vp, vp, i64, vp])
 _sig("qd_problem_solve", ci, [vp, ci, vp, vp])
 _sig("qd_coulomb", ci, [vp, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_last_timings", ci, [C.POINTER(C.c_double), ci])
+_sig("qd_tridiag_eigvals_noalloc", ci, [vp, ci, ci, ci, ci, vp, vp])
+_sig("qd_tridiag_bisect", ci, [vp, ci, ci, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_dev_alloc", ci, [C.c_size_t, C.POINTER(vp)])
 _sig("qd_dev_free", ci, [vp])
 _sig("qd_memcpy", ci, [vp, vp, C.c_size_t, ci])
