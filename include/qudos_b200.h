@@ -229,6 +229,24 @@ int qd_event_destroy(void *ev);
  * [4] inverse iteration, [5] back-transform, [6] refinement. */
 int qd_last_timings(double *ms, int n);
 
+/* Tensor-core building blocks of the mixed-precision reduction (tcgen05
+ * kind::tf32 with a 3xTF32 hi/lo split, FP32 accumulation), exposed for
+ * tests.  All pointers are device pointers to column-major complex64 data.
+ *   qd_tc_xprod: X[0:m, 0:nb] = A[off:off+m, off:off+m] * VT for a full
+ *     Hermitian n x n matrix A (lda even, off even), VT m x nb, nb <= 32.
+ *   qd_tc_flush: A[off:, off:] (mt x mt) -= P Q^H, P = [V W], Q = [W V]
+ *     with rows voff..voff+mt-1 and the first K columns of V and W.
+ * Work buffers serve matrices up to n rows and K <= kmax; qd_tc_work_check
+ * reports (and clears) a timed-out wait inside the kernels. */
+typedef struct QdTcWork QdTcWork;
+int qd_tc_work_alloc(int64_t n, int kmax, QdTcWork **out);
+void qd_tc_work_free(QdTcWork *w);
+int qd_tc_work_check(QdTcWork *w);
+int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, int m, const void *VT, int64_t ldvt, int nb,
+                void *X, int64_t ldx, QdTcWork *w, void *stream);
+int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void *V, const void *W, int64_t ldv, int64_t voff,
+                int K, QdTcWork *w, void *stream);
+
 /* Allocation-free eigenvalues of a Hermitian tridiagonal matrix for the index
  * window [lo, hi] (0-based, ascending), by the same Sturm-count multisection
  * as the solver's bisection stage.  No reference counterpart: it serves

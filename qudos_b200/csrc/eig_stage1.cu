@@ -240,6 +240,7 @@ static int n_panels(int64_t n, int b) {
 extern "C" cublasHandle_t qd_cublas(void);
 extern "C" int qd_mixed_gemm_mode(void);
 
+
 // typed cuBLAS wrappers --------------------------------------------------------
 template <typename T> struct Blas;
 template <> struct Blas<cuDoubleComplex> {
@@ -359,7 +360,9 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         T *X = Wacc + (off + b) + (int64_t)K * ldv;
         T *A22 = A + (k + b) + (k + b) * lda;
         BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, nb, &one, P, lda, Tp, b, &zero, VT, m));
-        if (full) {
+        if (full && w.tc) {
+            RC(qd_tc_xprod(A, lda, n, k + b, m, VT, m, nb, X, ldv, w.tc, st));
+        } else if (full) {
             BLAS_OK(Blas<T>::big(h, N_, N_, m, nb, m, &one, A22, lda, VT, m, &zero, X, ldv));
         } else {
             BLAS_OK(cublasZhemm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, m, nb, (const cuDoubleComplex *)&one,
@@ -390,7 +393,9 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
             int mt = (int)(n - kn);
             int64_t offn = kn - k0;
             T *At = A + kn + kn * lda;
-            if (full) {
+            if (full && w.tc) {
+                RC(qd_tc_flush(A, lda, kn, mt, Vacc, Wacc, ldv, offn, K, w.tc, st));
+            } else if (full) {
                 BLAS_OK(Blas<T>::big(h, N_, C_, mt, mt, K, &mone, Vacc + offn, ldv, Wacc + offn, ldv, &one, At, lda));
                 BLAS_OK(Blas<T>::big(h, N_, C_, mt, mt, K, &mone, Wacc + offn, ldv, Vacc + offn, ldv, &one, At, lda));
             } else {
@@ -408,6 +413,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
 }
 
 extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w) {
+    w->tc = nullptr;
     w->npanels = n_panels(n, b);
     const char *s = getenv("QD_AGG");
     int agg = s ? atoi(s) : 256;
@@ -431,6 +437,11 @@ extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w) 
         cudaMalloc(&w->bar, 4 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&w->err, sizeof(int)) != cudaSuccess)
         return qd_set_error(QD_ERR_NOMEM, "stage-1 scratch allocation failed");
     cudaMemset(w->err, 0, sizeof(int));
+    w->tc = nullptr;
+    if (elem_bytes == 8 && qd_mixed_gemm_mode() == 3 && (b % 2) == 0 && (n % 2) == 0) {
+        int rc = qd_tc_work_alloc(n, agg, &w->tc);
+        if (rc) return rc;
+    }
     return QD_OK;
 }
 
@@ -438,6 +449,8 @@ extern "C" void qd_stage1_free(Stage1Work *w) {
     void *p[] = {w->VT, w->X, w->M, w->Y, w->Tall, w->Rall, w->Vacc, w->Wacc, w->S1, w->S2, w->gram, w->tau,
                  w->red, w->rowbuf, w->bar, w->err};
     for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) cudaFree(p[i]);
+    if (w->tc) qd_tc_work_free(w->tc);
+    w->tc = nullptr;
 }
 
 extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, Stage1Work *w, void *stream) {
@@ -450,6 +463,7 @@ extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, S
     CUDA_OK(cudaMemcpyAsync(&herr, w->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
     if (herr) return qd_set_error(QD_ERR_TIMEOUT, "panel factorisation: grid barrier wait ran out");
+    if (w->tc) return qd_tc_work_check(w->tc);
     return QD_OK;
 }
 

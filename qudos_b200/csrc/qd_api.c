@@ -162,8 +162,10 @@ cublasHandle_t qd_cublas(void) {
 /* complex64 GEMM arithmetic of the mixed path: 2 = FP32 emulated with BF16x9 on
  * the tensor cores (default), 1 = TF32, 0 = plain FP32.  QD_MIXED_GEMM overrides. */
 int qd_mixed_gemm_mode(void) {
+    /* 3: the library's tcgen05 3xTF32 kernels; 0-2: cuBLAS CGEMM (FP32 SIMT,
+     * TF32, BF16x9 emulation) for comparison */
     const char *s = getenv("QD_MIXED_GEMM");
-    return s ? atoi(s) : 2;
+    return s ? atoi(s) : 3;
 }
 
 void qd_set_timing(int i, double ms);

@@ -93,6 +93,11 @@ _sig("qd_eigh_window_dev", ci, [i64, vp, i64, ci, ci, ci, vp, vp, i64, vp])
 _sig("qd_problem_solve", ci, [vp, ci, vp, vp])
 _sig("qd_coulomb", ci, [vp, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_last_timings", ci, [C.POINTER(C.c_double), ci])
+_sig("qd_tc_work_alloc", ci, [i64, ci, C.POINTER(vp)])
+_sig("qd_tc_work_free", None, [vp])
+_sig("qd_tc_work_check", ci, [vp])
+_sig("qd_tc_xprod", ci, [vp, i64, i64, i64, ci, vp, i64, ci, vp, i64, vp, vp])
+_sig("qd_tc_flush", ci, [vp, i64, i64, ci, vp, vp, i64, i64, ci, vp, vp])
 _sig("qd_tridiag_eigvals_noalloc", ci, [vp, ci, ci, ci, ci, vp, vp])
 _sig("qd_tridiag_bisect", ci, [vp, ci, ci, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_dev_alloc", ci, [C.c_size_t, C.POINTER(vp)])
