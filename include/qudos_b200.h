@@ -223,6 +223,9 @@ int qd_event_create(void **ev);
 int qd_event_record(void *ev, void *stream);
 int qd_event_elapsed_ms(void *ev0, void *ev1, float *ms);
 int qd_event_destroy(void *ev);
+/* The solve path keeps its device workspace in the device's stream-ordered
+ * memory pool between calls; this returns the cached memory to the driver. */
+int qd_trim_pool(void);
 
 /* Stage timings of the last qd_problem_solve / qd_eigh_window_dev call (ms):
  * [0] assembly, [1] band reduction, [2] bulge chasing, [3] bisection,

@@ -23,8 +23,8 @@
 
 typedef cpx<double> zd;
 
-extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w);
-extern "C" void qd_stage1_free(Stage1Work *w);
+extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, cudaStream_t st);
+extern "C" void qd_stage1_free(Stage1Work *w, cudaStream_t st);
 extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, Stage1Work *w, void *stream);
 extern "C" int qd_extract_band(const void *A, int64_t n, int64_t lda, int b, int fp32, const Stage1Work *w,
                                double2 *AB, int ldb, void *stream);
@@ -334,7 +334,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     int64_t lda = ld;
     float2 *H32 = nullptr;
     if (mixed) {
-        CUDA_OK(cudaMalloc(&H32, sizeof(float2) * n * n));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&H32, sizeof(float2) * n * n, st));
         qd_count_launch(1);
         lower64_to_full32_kernel<<<dim3((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)n), 256, 0, st>>>(
             (const double2 *)H, ld, n, H32, n);
@@ -343,21 +343,21 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         lda = n;
     }
     Stage1Work w1;
-    RC(qd_stage1_alloc(n, b, mixed ? 8 : 16, &w1));
+    RC(qd_stage1_alloc(n, b, mixed ? 8 : 16, &w1, st));
     RC(qd_stage1_run(A, n, lda, b, mixed, &w1, st));
     tm.mark();  // 1
     // ---- band, stage 2, bisection
     double2 *AB, *AB0, *Zb;
     double *d, *e2, *bounds, *lam;
     int *progress, *err;
-    CUDA_OK(cudaMalloc(&AB, sizeof(double2) * n * ldb));
-    CUDA_OK(cudaMalloc(&AB0, sizeof(double2) * n * ldb));
-    CUDA_OK(cudaMalloc(&d, sizeof(double) * n));
-    CUDA_OK(cudaMalloc(&e2, sizeof(double) * n));
-    CUDA_OK(cudaMalloc(&bounds, sizeof(double) * 4));
-    CUDA_OK(cudaMalloc(&lam, sizeof(double) * k));
-    CUDA_OK(cudaMalloc(&progress, sizeof(int) * n));
-    CUDA_OK(cudaMalloc(&err, sizeof(int)));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&AB, sizeof(double2) * n * ldb, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&AB0, sizeof(double2) * n * ldb, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&d, sizeof(double) * n, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&e2, sizeof(double) * n, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&bounds, sizeof(double) * 4, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&lam, sizeof(double) * k, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&progress, sizeof(int) * n, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&err, sizeof(int), st));
     RC(qd_extract_band(A, n, lda, b, mixed, &w1, AB, ldb, st));
     CUDA_OK(cudaMemcpyAsync(AB0, AB, sizeof(double2) * n * ldb, cudaMemcpyDeviceToDevice, st));
     RC(qd_hb2st(AB, ldb, (int)n, b, progress, err, st));
@@ -370,7 +370,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     std::vector<double> lam_h(k);
     CUDA_OK(cudaMemcpyAsync(lam_h.data(), lam, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
     unsigned long long *dmax;
-    CUDA_OK(cudaMalloc(&dmax, sizeof(unsigned long long)));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&dmax, sizeof(unsigned long long), st));
     CUDA_OK(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st));
     qd_count_launch(1);
     band_absmax_kernel<<<64, 256, 0, st>>>(AB0, ldb, n, b, dmax);
@@ -391,15 +391,15 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     int ng = (int)gs.size();
     int *gs_d, *gz_d, *ipiv;
     double2 *Lw, *Uw, *yw;
-    CUDA_OK(cudaMalloc(&gs_d, sizeof(int) * ng));
-    CUDA_OK(cudaMalloc(&gz_d, sizeof(int) * ng));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&gs_d, sizeof(int) * ng, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&gz_d, sizeof(int) * ng, st));
     CUDA_OK(cudaMemcpyAsync(gs_d, gs.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemcpyAsync(gz_d, gz.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMalloc(&Lw, sizeof(double2) * (size_t)ng * n * b));
-    CUDA_OK(cudaMalloc(&Uw, sizeof(double2) * (size_t)ng * n * (2 * b + 1)));
-    CUDA_OK(cudaMalloc(&ipiv, sizeof(int) * (size_t)ng * n));
-    CUDA_OK(cudaMalloc(&yw, sizeof(double2) * (size_t)ng * 8 * n));
-    CUDA_OK(cudaMalloc(&Zb, sizeof(double2) * n * k));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Lw, sizeof(double2) * (size_t)ng * n * b, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Uw, sizeof(double2) * (size_t)ng * n * (2 * b + 1), st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&ipiv, sizeof(int) * (size_t)ng * n, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&yw, sizeof(double2) * (size_t)ng * 8 * n, st));
+    CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Zb, sizeof(double2) * n * k, st));
     RC(qd_band_invit(AB0, ldb, (int)n, b, lam, ng, gs_d, gz_d, Lw, Uw, ipiv, Zb, n, bnorm, yw, st));
     tm.mark();  // 4
     // ---- back-transform
@@ -412,7 +412,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         tm.mark();  // 6
     } else {
         float2 *Z32;
-        CUDA_OK(cudaMalloc(&Z32, sizeof(float2) * n * k));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Z32, sizeof(float2) * n * k, st));
         qd_count_launch(4);
         c128_to_c64_kernel<<<dim3(64, k), 256, 0, st>>>(Zb, n, Z32, n, n);
         RC(qd_stage1_backtransform(A, n, lda, b, 1, &w1, Z32, n, k, st));
@@ -425,13 +425,13 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         double2 *Y, *S, *Ak, *C, *Xn;
         double *theta;
         int *info;
-        CUDA_OK(cudaMalloc(&Y, sizeof(double2) * n * k));
-        CUDA_OK(cudaMalloc(&Xn, sizeof(double2) * n * k));
-        CUDA_OK(cudaMalloc(&S, sizeof(double2) * k * k));
-        CUDA_OK(cudaMalloc(&Ak, sizeof(double2) * k * k));
-        CUDA_OK(cudaMalloc(&C, sizeof(double2) * k * k));
-        CUDA_OK(cudaMalloc(&theta, sizeof(double) * k));
-        CUDA_OK(cudaMalloc(&info, sizeof(int)));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Y, sizeof(double2) * n * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Xn, sizeof(double2) * n * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&S, sizeof(double2) * k * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Ak, sizeof(double2) * k * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&C, sizeof(double2) * k * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&theta, sizeof(double) * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&info, sizeof(int), st));
         CUDA_OK(cudaMemsetAsync(info, 0, sizeof(int), st));
         const cuDoubleComplex one = {1, 0}, zero = {0, 0};
         BLAS_OK(cublasZhemm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, (int)n, k, &one, (cuDoubleComplex *)H, (int)ld,
@@ -452,8 +452,8 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         CUDA_OK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
         tm.mark();  // 6
         CUDA_OK(cudaStreamSynchronize(st));
-        cudaFree(Y); cudaFree(Xn); cudaFree(S); cudaFree(Ak); cudaFree(C); cudaFree(theta); cudaFree(info);
-        cudaFree(Z32);
+        void *rr_bufs[] = {Y, Xn, S, Ak, C, theta, info, Z32};
+        for (void *p : rr_bufs) qd_pool_free(p, st);
         if (hinfo) return qd_set_error(QD_ERR_CONVERGENCE, "Rayleigh-Ritz: Gram matrix not positive definite");
     }
     CUDA_OK(cudaStreamSynchronize(st));
@@ -463,10 +463,9 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     g_timings[4] = tm.ms(3, 4);
     g_timings[5] = tm.ms(4, 5);
     g_timings[6] = tm.ms(5, 6);
-    cudaFree(AB); cudaFree(AB0); cudaFree(d); cudaFree(e2); cudaFree(bounds); cudaFree(lam); cudaFree(progress);
-    cudaFree(err); cudaFree(dmax); cudaFree(gs_d); cudaFree(gz_d); cudaFree(Lw); cudaFree(Uw); cudaFree(ipiv);
-    cudaFree(yw); cudaFree(Zb);
-    if (H32) cudaFree(H32);
-    qd_stage1_free(&w1);
+    void *bufs[] = {AB, AB0, d, e2, bounds, lam, progress, err, dmax, gs_d, gz_d, Lw, Uw, ipiv, yw, Zb, H32};
+    for (void *p : bufs)
+        if (p) qd_pool_free(p, st);
+    qd_stage1_free(&w1, st);
     return QD_OK;
 }

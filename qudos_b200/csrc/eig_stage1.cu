@@ -239,6 +239,8 @@ static int n_panels(int64_t n, int b) {
 
 extern "C" cublasHandle_t qd_cublas(void);
 extern "C" int qd_mixed_gemm_mode(void);
+extern "C" int qd_tc_work_alloc_on(int64_t n, int kmax, QdTcWork **out, cudaStream_t st);
+extern "C" void qd_tc_work_free_on(QdTcWork *w, cudaStream_t st);
 
 
 // typed cuBLAS wrappers --------------------------------------------------------
@@ -412,7 +414,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
     return QD_OK;
 }
 
-extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w) {
+extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, cudaStream_t st) {
     w->tc = nullptr;
     w->npanels = n_panels(n, b);
     const char *s = getenv("QD_AGG");
@@ -428,28 +430,29 @@ extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w) 
                       eb * (size_t)(w->npanels + 1) * b * b, eb * n * agg, eb * n * agg, eb * agg * b,
                       eb * agg * b, eb * b * b, eb * b};
     for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); i++)
-        if (cudaMalloc(bufs[i], sizes[i]) != cudaSuccess) return qd_set_error(QD_ERR_NOMEM, "stage-1 workspace");
+        if (qd_pool_alloc(bufs[i], sizes[i], st) != 0) return qd_set_error(QD_ERR_NOMEM, "stage-1 workspace");
     int dev, nsm;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaMalloc(&w->red, sizeof(double2) * 2 * (size_t)nsm * (b + 1)) != cudaSuccess ||
-        cudaMalloc(&w->rowbuf, sizeof(double2) * 2 * (size_t)b) != cudaSuccess ||
-        cudaMalloc(&w->bar, 4 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&w->err, sizeof(int)) != cudaSuccess)
+    if (qd_pool_alloc((void **)&w->red, sizeof(double2) * 2 * (size_t)nsm * (b + 1), st) != 0 ||
+        qd_pool_alloc((void **)&w->rowbuf, sizeof(double2) * 2 * (size_t)b, st) != 0 ||
+        qd_pool_alloc((void **)&w->bar, 4 * sizeof(unsigned), st) != 0 ||
+        qd_pool_alloc((void **)&w->err, sizeof(int), st) != 0)
         return qd_set_error(QD_ERR_NOMEM, "stage-1 scratch allocation failed");
-    cudaMemset(w->err, 0, sizeof(int));
+    CUDA_OK(cudaMemsetAsync(w->err, 0, sizeof(int), st));
     w->tc = nullptr;
     if (elem_bytes == 8 && qd_mixed_gemm_mode() == 3 && (b % 2) == 0 && (n % 2) == 0) {
-        int rc = qd_tc_work_alloc(n, agg, &w->tc);
+        int rc = qd_tc_work_alloc_on(n, agg, &w->tc, st);
         if (rc) return rc;
     }
     return QD_OK;
 }
 
-extern "C" void qd_stage1_free(Stage1Work *w) {
+extern "C" void qd_stage1_free(Stage1Work *w, cudaStream_t st) {
     void *p[] = {w->VT, w->X, w->M, w->Y, w->Tall, w->Rall, w->Vacc, w->Wacc, w->S1, w->S2, w->gram, w->tau,
                  w->red, w->rowbuf, w->bar, w->err};
-    for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) cudaFree(p[i]);
-    if (w->tc) qd_tc_work_free(w->tc);
+    for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) qd_pool_free(p[i], st);
+    if (w->tc) qd_tc_work_free_on(w->tc, st);
     w->tc = nullptr;
 }
 

@@ -61,6 +61,39 @@ static long long g_launches = 0;
 void qd_count_launch(int n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
 long long qd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
+/* Stream-ordered pool allocations of the solve path.  The first use on a
+ * device raises the release threshold of its default pool so that freed
+ * workspace stays mapped for the next solve; qd_trim_pool() hands it back. */
+static int g_pool_ready[64];
+int qd_pool_alloc(void **p, size_t bytes, void *stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev >= 0 && dev < 64 && !g_pool_ready[dev]) {
+        cudaMemPool_t pool;
+        e = cudaDeviceGetDefaultMemPool(&pool, dev);
+        if (e != cudaSuccess) return (int)e;
+        unsigned long long keep = ~0ull;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return (int)e;
+        g_pool_ready[dev] = 1;
+    }
+    return (int)cudaMallocAsync(p, bytes ? bytes : 16, (cudaStream_t)stream);
+}
+void qd_pool_free(void *p, void *stream) {
+    if (p) cudaFreeAsync(p, (cudaStream_t)stream);
+}
+int qd_trim_pool(void) {
+    int dev = 0;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, dev);
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "qd_trim_pool: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
 /* Device-memory, copy and event helpers so that callers without a CUDA
  * toolkit binding (ctypes, Fortran, ...) can drive the device-resident entry
  * points. */
@@ -351,9 +384,9 @@ int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *ei
     int M = pr->hi - pr->lo + 1;
     void *H = NULL, *Z = NULL;
     double *w = NULL;
-    CK(cudaMalloc(&H, sizeof(qd_complex128) * (size_t)n * (size_t)n));
-    CK(cudaMalloc(&Z, sizeof(qd_complex128) * (size_t)n * (size_t)M));
-    CK(cudaMalloc((void **)&w, sizeof(double) * (size_t)M));
+    CK((cudaError_t)qd_pool_alloc((void **)&H, sizeof(qd_complex128) * (size_t)n * (size_t)n, NULL));
+    CK((cudaError_t)qd_pool_alloc((void **)&Z, sizeof(qd_complex128) * (size_t)n * (size_t)M, NULL));
+    CK((cudaError_t)qd_pool_alloc((void **)&w, sizeof(double) * (size_t)M, NULL));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -372,9 +405,9 @@ int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *ei
             e = cudaMemcpy(eigvec, Z, sizeof(qd_complex128) * (size_t)n * (size_t)M, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "copy-out: %s", cudaGetErrorString(e));
     }
-    cudaFree(H);
-    cudaFree(Z);
-    cudaFree(w);
+    qd_pool_free(H, NULL);
+    qd_pool_free(Z, NULL);
+    qd_pool_free(w, NULL);
     return rc;
 }
 
@@ -452,7 +485,7 @@ void hamiltonian_8_band(int n_shape, struct vector F, struct wave_vectors basis,
     int64_t n = (int64_t)8 * basis.N_Gx * basis.N_Gy * basis.N_Gz;
     int64_t ld = na_rows > 0 ? na_rows : n;
     void *Hd = NULL;
-    if (rc == QD_OK && cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n) != cudaSuccess)
+    if (rc == QD_OK && qd_pool_alloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n, NULL) != 0)
         rc = qd_set_error(QD_ERR_NOMEM, "device H");
     if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, ld);
     /* copy the lower triangle column by column; the caller's strict upper triangle is left as it was */
@@ -461,7 +494,7 @@ void hamiltonian_8_band(int n_shape, struct vector F, struct wave_vectors basis,
                                    cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "copy-out: %s", cudaGetErrorString(e));
     }
-    if (Hd) cudaFree(Hd);
+    if (Hd) qd_pool_free(Hd, NULL);
     if (rc) die("hamiltonian_8_band", rc);
 }
 
@@ -472,9 +505,9 @@ void diagonalise_hamiltonian(int *idx_eig, qd_complex128 *H, double *eigval, qd_
     int lo = idx_eig[0] - 1, hi = idx_eig[1] - 1, M = hi - lo + 1;
     void *Hd = NULL, *Zd = NULL;
     double *wd = NULL;
-    if (rc == QD_OK && (cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n) != cudaSuccess ||
-                        cudaMalloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M) != cudaSuccess ||
-                        cudaMalloc((void **)&wd, sizeof(double) * (size_t)M) != cudaSuccess))
+    if (rc == QD_OK && (qd_pool_alloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n, NULL) != 0 ||
+                        qd_pool_alloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M, NULL) != 0 ||
+                        qd_pool_alloc((void **)&wd, sizeof(double) * (size_t)M, NULL) != 0))
         rc = qd_set_error(QD_ERR_NOMEM, "device buffers");
     if (rc == QD_OK && cudaMemcpy(Hd, H, sizeof(qd_complex128) * (size_t)ld * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
         rc = qd_set_error(QD_ERR_CUDA, "copy-in");
@@ -482,9 +515,9 @@ void diagonalise_hamiltonian(int *idx_eig, qd_complex128 *H, double *eigval, qd_
     if (rc == QD_OK && (cudaMemcpy(eigval, wd, sizeof(double) * (size_t)M, cudaMemcpyDeviceToHost) != cudaSuccess ||
                         cudaMemcpy(eigvec, Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M, cudaMemcpyDeviceToHost) != cudaSuccess))
         rc = qd_set_error(QD_ERR_CUDA, "copy-out");
-    cudaFree(Hd);
-    cudaFree(Zd);
-    cudaFree(wd);
+    qd_pool_free(Hd, NULL);
+    qd_pool_free(Zd, NULL);
+    qd_pool_free(wd, NULL);
     if (rc) die("diagonalise_hamiltonian", rc);
 }
 
@@ -497,9 +530,9 @@ void eigenstates(int n_shape, int *N_states, struct vector F, struct wave_vector
     int lo = idx_cb_min - 2 * N_states[0], hi = idx_cb_min + 2 * N_states[1] - 1, M = hi - lo + 1;
     void *Hd = NULL, *Zd = NULL;
     double *wd = NULL;
-    if (rc == QD_OK && (cudaMalloc(&Hd, sizeof(qd_complex128) * (size_t)n * (size_t)n) != cudaSuccess ||
-                        cudaMalloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M) != cudaSuccess ||
-                        cudaMalloc((void **)&wd, sizeof(double) * (size_t)M) != cudaSuccess))
+    if (rc == QD_OK && (qd_pool_alloc(&Hd, sizeof(qd_complex128) * (size_t)n * (size_t)n, NULL) != 0 ||
+                        qd_pool_alloc(&Zd, sizeof(qd_complex128) * (size_t)n * (size_t)M, NULL) != 0 ||
+                        qd_pool_alloc((void **)&wd, sizeof(double) * (size_t)M, NULL) != 0))
         rc = qd_set_error(QD_ERR_NOMEM, "device buffers");
     double t0 = wall_s();
     if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, n);
@@ -520,9 +553,9 @@ void eigenstates(int n_shape, int *N_states, struct vector F, struct wave_vector
             rc = qd_set_error(QD_ERR_CUDA, "copy-out");
     }
     free(w);
-    cudaFree(Hd);
-    cudaFree(Zd);
-    cudaFree(wd);
+    qd_pool_free(Hd, NULL);
+    qd_pool_free(Zd, NULL);
+    qd_pool_free(wd, NULL);
     if (rc) die("eigenstates", rc);
 }
 

@@ -55,6 +55,13 @@ void qd_basis_grid(int n_T, double L, double *out);
 
 void qd_count_launch(int n);
 
+/* Stream-ordered device allocations of the solve path, served from the
+ * device's default memory pool with its release threshold raised, so that
+ * repeated solves reuse the same memory instead of mapping it anew.
+ * Return cudaError_t values (0 = success). */
+int qd_pool_alloc(void **p, size_t bytes, void *stream);
+void qd_pool_free(void *p, void *stream);
+
 /* error state (api.cu) */
 int qd_set_error(int code, const char *fmt, ...);
 

@@ -3,7 +3,7 @@
 // operands staged by TMA with 128-byte swizzle).
 //
 // FP32 accuracy from TF32 inputs: every operand x is split into
-// hi = rna_tf32(x) and lo = rna_tf32(x - hi), and a*b is accumulated as
+// hi = tf32(x) and lo = tf32(x - hi) (round to nearest), and a*b is accumulated as
 // hi*hi + hi*lo + lo*hi in FP32 (the "3xTF32" split of Ootomo & Yokota 2022);
 // the neglected lo*lo term is ~2^-22 relative.
 //
@@ -18,13 +18,15 @@
 //                columns are read as K-major rows of conj(A22) = A22^T, so the
 //                big operand needs no transform; it is split hi/lo in shared
 //                memory by a converter warpgroup.  Split-K partials + reduce.
-//   qd_tc_flush  A22 -= [V W] [W V]^H (the aggregated rank-2K update); both
+//   qd_tc_flush  A22 -= [V W] [W V]^H (the aggregated rank-2K update) on the
+//                lower-triangle tiles, mirrored into the upper triangle; both
 //                factors are small and are laid out and split once per call.
 //
-// Kernel roles (one CTA per SM, persistent over output tiles):
-//   warp 0   TMA producer          warp 1   TMEM owner + MMA issuer
-//   warps 2-5 epilogue (TMEM -> registers -> global)
-//   warps 6-9 (xprod only) hi/lo converter of the streamed A tile
+// Both kernels are persistent (one CTA per SM) and warp-specialised: TMA
+// producer(s), one MMA-issuing thread that also owns TMEM, epilogue warps
+// that drain TMEM, and (xprod) a converter warpgroup.  The accumulator is
+// restarted every one or two k-blocks and summed in FP32 registers by the
+// epilogue, which keeps the tensor core's internal accumulation short.
 // Every mbarrier wait is bounded (about 2 s of %globaltimer); on a timeout
 // the kernel records an error code, stops issuing work, waits (bounded) for
 // its copies and MMAs in flight, frees its TMEM and returns.
@@ -48,36 +50,6 @@ namespace {
 constexpr int BKF = 32;  // floats per k-block row: 128 bytes = one SWIZZLE_128B atom
 constexpr int TILE_M = 128;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
-
-enum { MODE_XPROD = 0, MODE_FLUSH = 1 };
-
-template <int MODE> struct Cfg;
-template <> struct Cfg<MODE_XPROD> {
-    static constexpr int N = 64;  // 32 complex output columns
-    static constexpr int STAGES = 4;
-    static constexpr int A_BYTES = TILE_M * BKF * 4;
-    static constexpr int B_BYTES = N * BKF * 4;
-    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr int TX_BYTES = A_BYTES + 2 * B_BYTES;  // A_lo is written by the converter
-    static constexpr int EPI_WARPS = 4;                     // + 4 converter warps
-    static constexpr int EPI_COLS = 64;                     // TMEM columns per epilogue thread
-    static constexpr int CHUNK = 2;                         // k-blocks per TMEM accumulation chain
-    static constexpr int WARPS = 2 + EPI_WARPS + 4;
-    static constexpr int TMEM_COLS = 128;  // two accumulator buffers of N columns
-};
-template <> struct Cfg<MODE_FLUSH> {
-    static constexpr int N = 256;  // 128 complex output columns
-    static constexpr int STAGES = 2;
-    static constexpr int A_BYTES = TILE_M * BKF * 4;
-    static constexpr int B_BYTES = N * BKF * 4;
-    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr int TX_BYTES = STAGE_BYTES;
-    static constexpr int EPI_WARPS = 8;  // two warps per TMEM lane quarter, one per column half
-    static constexpr int EPI_COLS = 128;
-    static constexpr int CHUNK = 1;
-    static constexpr int WARPS = 2 + EPI_WARPS;
-    static constexpr int TMEM_COLS = 512;
-};
 
 struct TcArgs {
     int n_items, tiles_m, tiles_n, splits, kblocks;
@@ -180,63 +152,144 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+// Round to the nearest TF32 value (10 stored mantissa bits, ties away from
+// zero) with integer operations: add half an ulp of TF32 to the magnitude
+// bits and clear the 13 bits below.  Finite inputs far from FLT_MAX only.
+__device__ __forceinline__ float tf32_round(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
+// x = hi + lo with hi, lo TF32 values: hi carries 11 significant bits, the
+// exact remainder x - hi (|x - hi| <= 2^-11 |x|) is rounded again, so
+// |x - hi - lo| <= 2^-22 |x|.
 __device__ __forceinline__ void split3(float x, float &hi, float &lo) {
-    hi = tf32_rna(x);
-    lo = tf32_rna(x - hi);
+    hi = tf32_round(x);
+    lo = tf32_round(x - hi);
 }
 
-// item -> (tm, tn / split)
-__device__ __forceinline__ void item_coords(int MODEv, const TcArgs &a, int item, int &tm, int &tn, int &kb0,
-                                            int &kb1) {
-    if (MODEv == MODE_XPROD) {
-        tm = item % a.tiles_m;
-        tn = item / a.tiles_m;  // split index
-        kb0 = (int)((int64_t)tn * a.kblocks / a.splits);
-        kb1 = (int)((int64_t)(tn + 1) * a.kblocks / a.splits);
+// Lower-triangle tile (tm >= tn) of item `item` among T(T+1)/2, in bands of
+// 16 row tiles (column tiles outermost within a band) for L2 reuse of the
+// factor tiles.
+__device__ __forceinline__ void lower_tile(int item, int T, int &tm, int &tn) {
+    // items before band g (all bands before are full): 128 g^2 + 8 g
+    int g = (int)((-8.0 + sqrt(64.0 + 512.0 * (double)item)) / 256.0);
+    while (g > 0 && 128LL * g * g + 8LL * g > item) g--;
+    while (128LL * (g + 1) * (g + 1) + 8LL * (g + 1) <= item) g++;
+    int local = item - (128 * g * g + 8 * g);
+    int gs = min(16, T - 16 * g);
+    if (local < 16 * g * gs) {
+        tn = local / gs;
+        tm = 16 * g + local % gs;
     } else {
-        // bands of 16 row tiles, column tiles outermost within a band (L2 reuse)
-        const int G = 16;
-        int band = item / (G * a.tiles_n);
-        int local = item - band * G * a.tiles_n;
-        int gsz = min(G, a.tiles_m - band * G);
-        tm = band * G + local % gsz;
-        tn = local / gsz;
-        kb0 = 0;
-        kb1 = a.kblocks;
+        int t = local - 16 * g * gs, c = 0;
+        while (t >= gs - c) {
+            t -= gs - c;
+            c++;
+        }
+        tn = 16 * g + c;
+        tm = tn + t;
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmAlo,
-                   const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
-    typedef Cfg<MODE> K;
+__device__ __forceinline__ void xprod_item(const TcArgs &a, int item, int &tm, int &s, int &kb0, int &kb1) {
+    tm = item % a.tiles_m;
+    s = item / a.tiles_m;
+    kb0 = (int)((int64_t)s * a.kblocks / a.splits);
+    kb1 = (int)((int64_t)(s + 1) * a.kblocks / a.splits);
+}
+
+// Epilogue chunk loop shared by both kernels: drains every accumulation chunk
+// of one item from TMEM into FP32 registers.  Returns false on abort.
+template <int NCOLS, int ACC_COLS>
+__device__ __forceinline__ bool drain_item(float (&acc)[ACC_COLS], int nch, uint32_t tmem_base, int q, int cbase,
+                                           int &ab, uint32_t &aphase, uint64_t *tfull, uint64_t *tempty,
+                                           volatile int *abort_flag) {
+#pragma unroll
+    for (int c = 0; c < ACC_COLS; c++) acc[c] = 0.f;
+    for (int ch = 0; ch < nch; ch++) {
+        if (!mbar_wait(&tfull[ab], aphase, abort_flag)) return false;
+        tc_fence_after();
+#pragma unroll
+        for (int g = 0; g < ACC_COLS / 32; g++) {
+            uint32_t v[32];
+            tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * NCOLS + cbase + g * 32), v);
+#pragma unroll
+            for (int c = 0; c < 32; c++) acc[g * 32 + c] += __uint_as_float(v[c]);
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty[ab]);
+        if (++ab == 2) {
+            ab = 0;
+            aphase ^= 1;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void ring_next(int &s, uint32_t &ph, int n) {
+    if (++s == n) {
+        s = 0;
+        ph ^= 1;
+    }
+}
+__device__ __forceinline__ void ring_prev(int &s, uint32_t &ph, int n) {
+    if (--s < 0) {
+        s = n - 1;
+        ph ^= 1;
+    }
+}
+__device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
+    unsigned long long t0 = now_ns();
+    while (!mbar_try(bar, parity) && now_ns() - t0 < WAIT_NS) {
+    }
+}
+
+// ---------------------------------------------------------------------------
+// X = A22 VT.  Rings: A (TMA, fp32 -> hi in place) of XA_STAGES x 16 KB, and
+// work slots (lo of A, B hi, B lo) of XW_STAGES x 32 KB.
+//   warp 0 A producer, warp 1 MMA, warps 2-5 epilogue, warps 6-9 converter,
+//   warp 10 B producer.
+// ---------------------------------------------------------------------------
+constexpr int XA_STAGES = 7, XW_STAGES = 3;
+constexpr int X_N = 64;
+constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
+constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB
+constexpr int X_W_BYTES = X_A_BYTES + 2 * X_B_BYTES;
+constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XW_STAGES * X_W_BYTES;
+constexpr int X_CHUNK = 2;
+constexpr int X_WARPS = 11;
+constexpr int X_TMEM_COLS = 128;
+
+__global__ void __launch_bounds__(X_WARPS * 32, 1)
+    xprod_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = (uint64_t *)(smem + K::STAGES * K::STAGE_BYTES);
-    uint64_t *conv = full + K::STAGES;
-    uint64_t *empty = conv + K::STAGES;
-    uint64_t *tfull = empty + K::STAGES;  // [2]
-    uint64_t *tempty = tfull + 2;         // [2]
-    uint64_t *done = tempty + 2;          // [1]
+    uint8_t *ringA = smem, *ringW = smem + XA_STAGES * X_A_BYTES;
+    uint64_t *fullA = (uint64_t *)(smem + X_SMEM);
+    uint64_t *emptyA = fullA + XA_STAGES;
+    uint64_t *fullB = emptyA + XA_STAGES;
+    uint64_t *conv = fullB + XW_STAGES;
+    uint64_t *emptyW = conv + XW_STAGES;
+    uint64_t *tfull = emptyW + XW_STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *done = tempty + 2;
     uint32_t *tmem_slot = (uint32_t *)(done + 1);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < K::STAGES; s++) {
-            mbar_init(&full[s], 1);
+        for (int s = 0; s < XA_STAGES; s++) {
+            mbar_init(&fullA[s], 1);
+            mbar_init(&emptyA[s], 1);
+        }
+        for (int s = 0; s < XW_STAGES; s++) {
+            mbar_init(&fullB[s], 1);
             mbar_init(&conv[s], 128);
-            mbar_init(&empty[s], 1);
+            mbar_init(&emptyW[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], K::EPI_WARPS * 32);
+            mbar_init(&tempty[b], 128);
         }
         mbar_init(done, 1);
         *abort_flag = 0;
@@ -244,7 +297,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"((uint32_t)K::TMEM_COLS)
+                     "r"((uint32_t)X_TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -252,81 +305,61 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-
     auto fail = [&](int code) {
         atomicCAS(args.err, 0, code);
         *abort_flag = 1;
     };
 
-    if (warp == 0) {
-        // ---------------- TMA producer ----------------
+    if (warp == 0 || warp == 10) {
+        // ---------------- producers: A ring (warp 0), B into work slots (warp 10) ----------------
         if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
+            const bool isA = warp == 0;
+            const int nst = isA ? XA_STAGES : XW_STAGES;
+            int s = 0;
+            uint32_t ph = 0;
             long issued = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
-                int tm, tn, kb0, kb1;
-                item_coords(MODE, args, item, tm, tn, kb0, kb1);
+                int tm, sp, kb0, kb1;
+                xprod_item(args, item, tm, sp, kb0, kb1);
                 for (int kb = kb0; kb < kb1; kb++) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
-                        fail(1);
+                    if (!mbar_wait(isA ? &emptyA[s] : &emptyW[s], ph ^ 1, abort_flag)) {
+                        fail(isA ? 1 : 6);
                         ok = false;
                         break;
                     }
-                    uint8_t *sA = smem + stage * K::STAGE_BYTES;
-                    uint8_t *sAlo = sA + K::A_BYTES;
-                    uint8_t *sB = sAlo + K::A_BYTES;
-                    uint8_t *sBlo = sB + K::B_BYTES;
-                    mbar_expect_tx(&full[stage], K::TX_BYTES);
-                    int x = kb * BKF;
-                    if (MODE == MODE_XPROD) {
-                        tma_load_2d(&tmA, &full[stage], sA, args.a_x0 + x, args.a_y0 + tm * TILE_M);
-                        tma_load_2d(&tmB, &full[stage], sB, x, 0);
-                        tma_load_2d(&tmBlo, &full[stage], sBlo, x, 0);
+                    if (isA) {
+                        mbar_expect_tx(&fullA[s], X_A_BYTES);
+                        tma_load_2d(&tmA, &fullA[s], ringA + s * X_A_BYTES, args.a_x0 + kb * BKF,
+                                    args.a_y0 + tm * TILE_M);
                     } else {
-                        tma_load_2d(&tmA, &full[stage], sA, x, tm * TILE_M);
-                        tma_load_2d(&tmAlo, &full[stage], sAlo, x, tm * TILE_M);
-                        tma_load_2d(&tmB, &full[stage], sB, x, tn * K::N);
-                        tma_load_2d(&tmBlo, &full[stage], sBlo, x, tn * K::N);
+                        uint8_t *w = ringW + s * X_W_BYTES;
+                        mbar_expect_tx(&fullB[s], 2 * X_B_BYTES);
+                        tma_load_2d(&tmB, &fullB[s], w + X_A_BYTES, kb * BKF, 0);
+                        tma_load_2d(&tmBlo, &fullB[s], w + X_A_BYTES + X_B_BYTES, kb * BKF, 0);
                     }
                     issued++;
-                    if (++stage == K::STAGES) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
+                    ring_next(s, ph, nst);
                 }
             }
-            // wait for the copies still in flight (all consumed already on the normal path)
-            long outstanding = issued < K::STAGES ? issued : K::STAGES;
+            long outstanding = issued < nst ? issued : nst;
             for (long q = 0; q < outstanding; q++) {
-                if (--stage < 0) {
-                    stage = K::STAGES - 1;
-                    phase ^= 1;
-                }
-                unsigned long long t0 = now_ns();
-                while (!mbar_try(&full[stage], phase) && now_ns() - t0 < WAIT_NS) {
-                }
+                ring_prev(s, ph, nst);
+                wait_bounded(isA ? &fullA[s] : &fullB[s], ph);
             }
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        // The accumulator is restarted every CHUNK k-blocks and drained by the
-        // epilogue into FP32 registers: the tensor core's own accumulation
-        // then only spans 12*CHUNK MMAs, which keeps its rounding error near
-        // that of an FP32 dot product.
+        // ---------------- MMA issuer (accumulation restarted every X_CHUNK k-blocks) ----------------
         if (lane == 0) {
-            const uint32_t idesc = tf32_idesc(TILE_M, K::N);
-            int stage = 0;
-            uint32_t phase = 0;
-            int ab = 0;
-            uint32_t aphase = 0;
+            const uint32_t idesc = tf32_idesc(TILE_M, X_N);
+            int sa = 0, sw = 0, ab = 0;
+            uint32_t pa = 0, pw = 0, aphase = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
-                int tm, tn, kb0, kb1;
-                item_coords(MODE, args, item, tm, tn, kb0, kb1);
+                int tm, sp, kb0, kb1;
+                xprod_item(args, item, tm, sp, kb0, kb1);
                 for (int kb = kb0; kb < kb1; kb++) {
-                    const int cpos = (kb - kb0) % K::CHUNK;
+                    const int cpos = (kb - kb0) % X_CHUNK;
                     if (cpos == 0) {
                         if (!mbar_wait(&tempty[ab], aphase ^ 1, abort_flag)) {
                             fail(2);
@@ -335,32 +368,29 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
                         }
                         tc_fence_after();
                     }
-                    if (!mbar_wait(&full[stage], phase, abort_flag) ||
-                        (MODE == MODE_XPROD && !mbar_wait(&conv[stage], phase, abort_flag))) {
+                    if (!mbar_wait(&fullB[sw], pw, abort_flag) || !mbar_wait(&conv[sw], pw, abort_flag)) {
                         fail(3);
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d = tmem_base + (uint32_t)(ab * K::N);
-                    uint32_t a_hi = smem_u32(smem + stage * K::STAGE_BYTES);
-                    uint32_t a_lo = a_hi + K::A_BYTES;
-                    uint32_t b_hi = a_lo + K::A_BYTES;
-                    uint32_t b_lo = b_hi + K::B_BYTES;
+                    const uint32_t d = tmem_base + (uint32_t)(ab * X_N);
+                    const uint32_t a_hi = smem_u32(ringA + sa * X_A_BYTES);
+                    const uint32_t a_lo = smem_u32(ringW + sw * X_W_BYTES);
+                    const uint32_t b_hi = a_lo + X_A_BYTES, b_lo = b_hi + X_B_BYTES;
 #pragma unroll
-                    for (int kk = 0; kk < BKF / 8; kk++) {  // 8 tf32 = 32 bytes per MMA
+                    for (int kk = 0; kk < BKF / 8; kk++) {
                         uint32_t o = kk * 32;
                         uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
                         umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_hi + o), idesc, acc);
                         umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_lo + o), idesc, 1u);
                         umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
                     }
-                    umma_commit(&empty[stage]);
-                    if (++stage == K::STAGES) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
-                    if (cpos == K::CHUNK - 1 || kb == kb1 - 1) {
+                    umma_commit(&emptyA[sa]);
+                    umma_commit(&emptyW[sw]);
+                    ring_next(sa, pa, XA_STAGES);
+                    ring_next(sw, pw, XW_STAGES);
+                    if (cpos == X_CHUNK - 1 || kb == kb1 - 1) {
                         umma_commit(&tfull[ab]);
                         if (++ab == 2) {
                             ab = 0;
@@ -369,90 +399,49 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
                     }
                 }
             }
-            // all MMAs issued by this thread complete before TMEM is released
             umma_commit(done);
-            unsigned long long t0 = now_ns();
-            while (!mbar_try(done, 0) && now_ns() - t0 < WAIT_NS) {
-            }
+            wait_bounded(done, 0);
         }
-    } else if (warp < 2 + K::EPI_WARPS) {
-        // ---------------- epilogue: drain each chunk, sum in FP32 registers ----------------
-        const int q = warp & 3;                                 // TMEM lane quarter this warp may access
-        const int cbase = ((warp - 2) >> 2) * K::EPI_COLS;    // TMEM column range of this warp
-        const int r = q * 32 + lane;
+    } else if (warp < 6) {
+        // ---------------- epilogue: split-K partials ----------------
+        const int q = warp & 3, r = q * 32 + lane;
         int ab = 0;
         uint32_t aphase = 0;
-        bool ok = true;
-        for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
-            int tm, tn, kb0, kb1;
-            item_coords(MODE, args, item, tm, tn, kb0, kb1);
-            float acc[K::EPI_COLS];
-#pragma unroll
-            for (int c = 0; c < K::EPI_COLS; c++) acc[c] = 0.f;
-            const int nch = (kb1 - kb0 + K::CHUNK - 1) / K::CHUNK;
-            for (int ch = 0; ch < nch; ch++) {
-                if (!mbar_wait(&tfull[ab], aphase, abort_flag)) {
-                    fail(4);
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-#pragma unroll
-                for (int g = 0; g < K::EPI_COLS / 32; g++) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * K::N + cbase + g * 32), v);
-#pragma unroll
-                    for (int c = 0; c < 32; c++) acc[g * 32 + c] += __uint_as_float(v[c]);
-                }
-                tc_fence_before();
-                mbar_arrive(&tempty[ab]);
-                if (++ab == 2) {
-                    ab = 0;
-                    aphase ^= 1;
-                }
+        for (int item = blockIdx.x; item < args.n_items; item += gridDim.x) {
+            int tm, sp, kb0, kb1;
+            xprod_item(args, item, tm, sp, kb0, kb1);
+            float acc[X_N];
+            if (!drain_item<X_N, X_N>(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, 0, ab, aphase, tfull,
+                                      tempty, abort_flag)) {
+                fail(4);
+                break;
             }
-            if (!ok) break;
             const int row = tm * TILE_M + r;
             if (row < args.rows) {
-                if (MODE == MODE_XPROD) {
-                    float2 *Xp = args.C + (int64_t)tn * args.ldc * 32;
+                float2 *Xp = args.C + (int64_t)sp * args.ldc * 32;
 #pragma unroll
-                    for (int l = 0; l < 32; l++)
-                        Xp[row + (int64_t)l * args.ldc] = make_float2(acc[2 * l], acc[2 * l + 1]);
-                } else {
-#pragma unroll
-                    for (int jj = 0; jj < K::EPI_COLS / 2; jj++) {
-                        int col = tn * (K::N / 2) + cbase / 2 + jj;
-                        if (col < args.cols) {
-                            float2 *p = args.C + row + (int64_t)col * args.ldc;
-                            float2 c = *p;
-                            c.x -= acc[2 * jj];
-                            c.y -= acc[2 * jj + 1];
-                            *p = c;
-                        }
-                    }
-                }
+                for (int l = 0; l < 32; l++) Xp[row + (int64_t)l * args.ldc] = make_float2(acc[2 * l], acc[2 * l + 1]);
             }
         }
-    } else if (MODE == MODE_XPROD) {
-        // ---------------- hi/lo converter of the streamed A tile ----------------
-        const int t = threadIdx.x - (2 + K::EPI_WARPS) * 32;  // 0..127
-        int stage = 0;
-        uint32_t phase = 0;
+    } else {
+        // ---------------- converter: A fp32 -> hi (in place) + lo (work slot) ----------------
+        const int t = threadIdx.x - 6 * 32;  // 0..127
+        int sa = 0, sw = 0;
+        uint32_t pa = 0, pw = 0;
         bool ok = true;
         for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
-            int tm, tn, kb0, kb1;
-            item_coords(MODE, args, item, tm, tn, kb0, kb1);
+            int tm, sp, kb0, kb1;
+            xprod_item(args, item, tm, sp, kb0, kb1);
             for (int kb = kb0; kb < kb1; kb++) {
-                if (!mbar_wait(&full[stage], phase, abort_flag)) {
+                if (!mbar_wait(&fullA[sa], pa, abort_flag) || !mbar_wait(&emptyW[sw], pw ^ 1, abort_flag)) {
                     fail(5);
                     ok = false;
                     break;
                 }
-                float4 *a = (float4 *)(smem + stage * K::STAGE_BYTES);
-                float4 *alo = (float4 *)(smem + stage * K::STAGE_BYTES + K::A_BYTES);
+                float4 *a = (float4 *)(ringA + sa * X_A_BYTES);
+                float4 *alo = (float4 *)(ringW + sw * X_W_BYTES);
 #pragma unroll
-                for (int u = 0; u < K::A_BYTES / 16 / 128; u++) {
+                for (int u = 0; u < X_A_BYTES / 16 / 128; u++) {
                     int idx = u * 128 + t;
                     float4 x = a[idx], h, l;
                     split3(x.x, h.x, l.x);
@@ -463,10 +452,182 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
                     alo[idx] = l;
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(&conv[stage]);
-                if (++stage == K::STAGES) {
-                    stage = 0;
-                    phase ^= 1;
+                mbar_arrive(&conv[sw]);
+                ring_next(sa, pa, XA_STAGES);
+                ring_next(sw, pw, XW_STAGES);
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"((uint32_t)X_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C -= P Q^H on the lower-triangle tiles of the Hermitian trailing matrix;
+// the strictly upper part is written as the conjugate transpose (so the
+// stored matrix stays exactly Hermitian) and diagonal entries stay real.
+//   warp 0 producer, warp 1 MMA, warps 2-9 epilogue (two per lane quarter).
+// ---------------------------------------------------------------------------
+constexpr int F_STAGES = 2;
+constexpr int F_N = 256;
+constexpr int F_A_BYTES = TILE_M * BKF * 4;  // 16 KB
+constexpr int F_B_BYTES = F_N * BKF * 4;     // 32 KB
+constexpr int F_STAGE_BYTES = 2 * F_A_BYTES + 2 * F_B_BYTES;
+constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES;
+constexpr int F_EPI_COLS = 128;
+constexpr int F_WARPS = 10;
+constexpr int F_TMEM_COLS = 512;
+
+__global__ void __launch_bounds__(F_WARPS * 32, 1)
+    flush_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmAlo,
+                 const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + F_SMEM);
+    uint64_t *empty = full + F_STAGES;
+    uint64_t *tfull = empty + F_STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *done = tempty + 2;
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+    volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int T = args.tiles_m;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < F_STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 256);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)F_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    auto fail = [&](int code) {
+        atomicCAS(args.err, 0, code);
+        *abort_flag = 1;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            long issued = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
+                int tm, tn;
+                lower_tile(item, T, tm, tn);
+                for (int kb = 0; kb < args.kblocks; kb++) {
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) {
+                        fail(1);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *st = smem + s * F_STAGE_BYTES;
+                    mbar_expect_tx(&full[s], F_STAGE_BYTES);
+                    int x = kb * BKF;
+                    tma_load_2d(&tmA, &full[s], st, x, tm * TILE_M);
+                    tma_load_2d(&tmAlo, &full[s], st + F_A_BYTES, x, tm * TILE_M);
+                    tma_load_2d(&tmB, &full[s], st + 2 * F_A_BYTES, x, tn * F_N);
+                    tma_load_2d(&tmBlo, &full[s], st + 2 * F_A_BYTES + F_B_BYTES, x, tn * F_N);
+                    issued++;
+                    ring_next(s, ph, F_STAGES);
+                }
+            }
+            long outstanding = issued < F_STAGES ? issued : F_STAGES;
+            for (long q = 0; q < outstanding; q++) {
+                ring_prev(s, ph, F_STAGES);
+                wait_bounded(&full[s], ph);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tf32_idesc(TILE_M, F_N);
+            int s = 0, ab = 0;
+            uint32_t ph = 0, aphase = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
+                for (int kb = 0; kb < args.kblocks; kb++) {  // one k-block per accumulation chunk
+                    if (!mbar_wait(&tempty[ab], aphase ^ 1, abort_flag) || !mbar_wait(&full[s], ph, abort_flag)) {
+                        fail(3);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + (uint32_t)(ab * F_N);
+                    const uint32_t a_hi = smem_u32(smem + s * F_STAGE_BYTES);
+                    const uint32_t a_lo = a_hi + F_A_BYTES, b_hi = a_lo + F_A_BYTES, b_lo = b_hi + F_B_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < BKF / 8; kk++) {
+                        uint32_t o = kk * 32;
+                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_hi + o), idesc, kk > 0 ? 1u : 0u);
+                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_lo + o), idesc, 1u);
+                        umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
+                    }
+                    umma_commit(&empty[s]);
+                    umma_commit(&tfull[ab]);
+                    ring_next(s, ph, F_STAGES);
+                    if (++ab == 2) {
+                        ab = 0;
+                        aphase ^= 1;
+                    }
+                }
+            }
+            umma_commit(done);
+            wait_bounded(done, 0);
+        }
+    } else {
+        const int q = warp & 3, r = q * 32 + lane;
+        const int cbase = ((warp - 2) >> 2) * F_EPI_COLS;
+        int ab = 0;
+        uint32_t aphase = 0;
+        for (int item = blockIdx.x; item < args.n_items; item += gridDim.x) {
+            int tm, tn;
+            lower_tile(item, T, tm, tn);
+            float acc[F_EPI_COLS];
+            if (!drain_item<F_N, F_EPI_COLS>(acc, args.kblocks, tmem_base, q, cbase, ab, aphase, tfull, tempty,
+                                             abort_flag)) {
+                fail(4);
+                break;
+            }
+            const int row = tm * TILE_M + r;
+            if (row >= args.rows) continue;
+            float2 *Crow = args.C + row;                            // C[row, :]
+            float2 *Ccol = args.C + (int64_t)row * args.ldc;        // C[:, row] (mirror)
+            const int col0 = tn * (F_N / 2) + cbase / 2;
+#pragma unroll
+            for (int jj = 0; jj < F_EPI_COLS / 2; jj++) {
+                const int col = col0 + jj;
+                if (col >= args.cols || col > row) continue;
+                float2 *p = Crow + (int64_t)col * args.ldc;
+                float2 c = *p;
+                c.x -= acc[2 * jj];
+                c.y -= acc[2 * jj + 1];
+                if (col == row) {
+                    c.y = 0.f;
+                    *p = c;
+                } else {
+                    *p = c;
+                    Ccol[col] = make_float2(c.x, -c.y);
                 }
             }
         }
@@ -476,8 +637,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::WARPS * 32, 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"((uint32_t)K::TMEM_COLS)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"((uint32_t)F_TMEM_COLS)
                      : "memory");
     }
 }
@@ -608,24 +768,36 @@ int sm_count() {
     return g_nsm;
 }
 
-template <int MODE>
-int smem_bytes() {
-    return Cfg<MODE>::STAGES * Cfg<MODE>::STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-}
+constexpr int SMEM_EXTRA = 1024 /*alignment*/ + 256 /*barriers*/;
 
-template <int MODE>
-int launch(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap &b, const CUtensorMap &blo,
-           const TcArgs &args, cudaStream_t st) {
+int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &blo, const TcArgs &args,
+                 cudaStream_t st) {
     static bool configured = false;
-    int smem = smem_bytes<MODE>();
+    const int smem = X_SMEM + SMEM_EXTRA;
     if (!configured) {
-        CUDA_OK(cudaFuncSetAttribute(tc_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_OK(cudaFuncSetAttribute(xprod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         configured = true;
     }
     int grid = args.n_items < sm_count() ? args.n_items : sm_count();
     if (grid < 1) return QD_OK;
     qd_count_launch(1);
-    tc_gemm_kernel<MODE><<<grid, Cfg<MODE>::WARPS * 32, smem, st>>>(a, alo, b, blo, args);
+    xprod_kernel<<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
+    CUDA_OK(cudaGetLastError());
+    return QD_OK;
+}
+
+int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap &b, const CUtensorMap &blo,
+                 const TcArgs &args, cudaStream_t st) {
+    static bool configured = false;
+    const int smem = F_SMEM + SMEM_EXTRA;
+    if (!configured) {
+        CUDA_OK(cudaFuncSetAttribute(flush_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        configured = true;
+    }
+    int grid = args.n_items < sm_count() ? args.n_items : sm_count();
+    if (grid < 1) return QD_OK;
+    qd_count_launch(1);
+    flush_kernel<<<grid, F_WARPS * 32, smem, st>>>(a, alo, b, blo, args);
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }
@@ -634,6 +806,8 @@ int launch(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap &b, c
 
 // Work buffers of the tensor-core path (device), sized for an n x n matrix
 // and rank-2K updates with K <= kmax.
+extern "C" void qd_tc_work_free_on(struct QdTcWork *w, cudaStream_t st);
+
 struct QdTcWork {
     float *bx_hi, *bx_lo;  // 64 x pitch_x
     int64_t pitch_x;
@@ -646,7 +820,7 @@ struct QdTcWork {
     int *err;
 };
 
-extern "C" int qd_tc_work_alloc(int64_t n, int kmax, QdTcWork **out) {
+extern "C" int qd_tc_work_alloc_on(int64_t n, int kmax, QdTcWork **out, cudaStream_t st) {
     QdTcWork *w = (QdTcWork *)calloc(1, sizeof(QdTcWork));
     if (!w) return qd_set_error(QD_ERR_NOMEM, "qd_tc_work_alloc");
     w->n = n;
@@ -658,40 +832,35 @@ extern "C" int qd_tc_work_alloc(int64_t n, int kmax, QdTcWork **out) {
     size_t xp = sizeof(float2) * 32 * (size_t)w->ldp * w->max_splits;
     size_t fa = sizeof(float) * (size_t)n * 4 * kmax;
     size_t fb = 2 * fa;
-    void *p[7] = {nullptr};
-    size_t sz[7] = {bx, bx, xp, fa, fa, fb, fb};
-    for (int i = 0; i < 7; i++) {
-        if (cudaMalloc(&p[i], sz[i]) != cudaSuccess) {
-            for (int k = 0; k < i; k++) cudaFree(p[k]);
-            free(w);
-            cudaGetLastError();
-            return qd_set_error(QD_ERR_NOMEM, "qd_tc_work_alloc: %zu bytes", sz[i]);
+    void **dst[8] = {(void **)&w->bx_hi, (void **)&w->bx_lo, (void **)&w->xp, (void **)&w->fa_hi,
+                     (void **)&w->fa_lo, (void **)&w->fb_hi, (void **)&w->fb_lo, (void **)&w->err};
+    size_t sz[8] = {bx, bx, xp, fa, fa, fb, fb, sizeof(int)};
+    for (int i = 0; i < 8; i++) {
+        if (qd_pool_alloc(dst[i], sz[i], st) != 0) {
+            qd_tc_work_free_on(w, st);
+            return qd_set_error(QD_ERR_NOMEM, "tensor-core work buffers: %zu bytes", sz[i]);
         }
     }
-    w->bx_hi = (float *)p[0];
-    w->bx_lo = (float *)p[1];
-    w->xp = (float2 *)p[2];
-    w->fa_hi = (float *)p[3];
-    w->fa_lo = (float *)p[4];
-    w->fb_hi = (float *)p[5];
-    w->fb_lo = (float *)p[6];
-    if (cudaMalloc(&w->err, sizeof(int)) != cudaSuccess) {
-        for (int k = 0; k < 7; k++) cudaFree(p[k]);
-        free(w);
-        return qd_set_error(QD_ERR_NOMEM, "qd_tc_work_alloc");
-    }
-    cudaMemset(w->err, 0, sizeof(int));
+    CUDA_OK(cudaMemsetAsync(w->err, 0, sizeof(int), st));
     *out = w;
     return QD_OK;
 }
 
-extern "C" void qd_tc_work_free(QdTcWork *w) {
+extern "C" void qd_tc_work_free_on(QdTcWork *w, cudaStream_t st) {
     if (!w) return;
     void *p[8] = {w->bx_hi, w->bx_lo, w->xp, w->fa_hi, w->fa_lo, w->fb_hi, w->fb_lo, w->err};
     for (int i = 0; i < 8; i++)
-        if (p[i]) cudaFree(p[i]);
+        if (p[i]) qd_pool_free(p[i], st);
     free(w);
 }
+
+extern "C" int qd_tc_work_alloc(int64_t n, int kmax, QdTcWork **out) {
+    int rc = qd_tc_work_alloc_on(n, kmax, out, 0);
+    if (rc == QD_OK) CUDA_OK(cudaStreamSynchronize(0));
+    return rc;
+}
+
+extern "C" void qd_tc_work_free(QdTcWork *w) { qd_tc_work_free_on(w, 0); }
 
 // Error code left by the tensor-core kernels (0 = none); clears it.
 extern "C" int qd_tc_work_check(QdTcWork *w) {
@@ -742,7 +911,7 @@ extern "C" int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, i
     a.ldc = w->ldp;
     a.err = w->err;
     if (m > w->ldp) return qd_set_error(QD_ERR_ARG, "qd_tc_xprod: m exceeds the work buffers");
-    if ((rc = launch<MODE_XPROD>(ta, ta, tb, tblo, a, st))) return rc;
+    if ((rc = launch_xprod(ta, tb, tblo, a, st))) return rc;
     qd_count_launch(1);
     reduce_splits_kernel<<<dim3((unsigned)((m + 127) / 128), nb), 128, 0, st>>>(w->xp, w->ldp, splits, m, nb,
                                                                                   (float2 *)X, ldx);
@@ -771,10 +940,10 @@ extern "C" int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void
     if ((rc = make_map(&tblo, w->fb_lo, (uint64_t)pitch, 2 * (uint64_t)mt, (uint64_t)pitch * 4, 256))) return rc;
     TcArgs a;
     a.tiles_m = (mt + TILE_M - 1) / TILE_M;
-    a.tiles_n = (mt + 127) / 128;
+    a.tiles_n = a.tiles_m;
     a.splits = 1;
     a.kblocks = (int)((pitch + BKF - 1) / BKF);
-    a.n_items = a.tiles_m * a.tiles_n;
+    a.n_items = a.tiles_m * (a.tiles_m + 1) / 2;  // lower-triangle tiles
     a.rows = mt;
     a.cols = mt;
     a.a_x0 = 0;
@@ -782,5 +951,5 @@ extern "C" int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void
     a.C = (float2 *)A + off + off * lda;
     a.ldc = lda;
     a.err = w->err;
-    return launch<MODE_FLUSH>(ta, talo, tb, tblo, a, st);
+    return launch_flush(ta, talo, tb, tblo, a, st);
 }
