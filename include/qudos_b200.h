@@ -200,11 +200,15 @@ int qd_eigh_window_dev(int64_t n, void *H_dev, int64_t ld, int lo, int hi, int p
  * eigensolve; eigval (M) and eigvec (N_H x M) in host memory. */
 int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *eigvec);
 
-/* Coulomb matrix elements (include_CME = 1 physics) for M_c states
- * (eigvec_host: N_H x M_c, first 2 N_vb VB states then 2 N_cb CB states) into
- * the reference's four output arrays (sizes of 8_band_main.c:1752-1755). */
+/* Coulomb matrix elements (coulomb_matrix_elements.c:24, free Coulomb-cell
+ * lengths, the problem's CME setting 1..4) for n_vb_states + n_cb_states
+ * states (eigvec_host: N_H x M_c, VB states first, as eigenstates orders
+ * them) into the reference's four arrays (sizes of 8_band_main.c:1752-1755;
+ * elements outside the reference's computed set are zero).  The real-space
+ * part of the Madelung sum follows the reference's split over
+ * madelung_ranks MPI ranks (its value depends on the rank count). */
 int qd_coulomb(qd_problem *pr, int n_vb_states, int n_cb_states, const qd_complex128 *eigvec_host,
-               qd_complex128 *hh, qd_complex128 *ee, qd_complex128 *eh_direct,
+               int madelung_ranks, qd_complex128 *hh, qd_complex128 *ee, qd_complex128 *eh_direct,
                qd_complex128 *eh_exchange);
 
 /* Device plumbing for callers without their own CUDA binding.  qd_memcpy kind:
@@ -231,6 +235,11 @@ int qd_trim_pool(void);
  * [0] assembly, [1] band reduction, [2] bulge chasing, [3] bisection,
  * [4] inverse iteration, [5] back-transform, [6] refinement. */
 int qd_last_timings(double *ms, int n);
+/* With QD_PROFILE=1 in the environment: per-step times (ms) of the last
+ * dense->band reduction: [0] panel refresh, [1] panel QR, [2] T and V T,
+ * [3] X = A22 V T, [4] pending-update corrections, [5] W, [6] append,
+ * [7] trailing rank-2K updates.  Adds one event per step boundary. */
+int qd_stage1_profile(double *ms, int n);
 
 /* Tensor-core building blocks of the mixed-precision reduction (tcgen05
  * kind::tf32 with a 3xTF32 hi/lo split, FP32 accumulation), exposed for

@@ -26,6 +26,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <vector>
+
 #include "eig_common.cuh"
 #include "qd_internal.h"
 
@@ -322,6 +324,54 @@ static int launch_panel(T *P, int64_t lda, int m, int nb, int nref, T *Rp, T *ta
 }
 
 // Stage 1 for element type T (cuDoubleComplex: lower triangle; cuComplex: full matrix).
+// Opt-in breakdown of the reduction (QD_PROFILE=1): events recorded at the
+// boundaries of the steps of every panel, summed per step after the stage.
+// Steps: 0 panel refresh, 1 panel QR, 2 T and VT, 3 X = A22 VT,
+// 4 pending-update corrections, 5 W, 6 append, 7 trailing update.
+namespace {
+struct StageProfile {
+    int on = -1;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> step;
+    int used = 0;
+    double ms[8] = {0};
+};
+StageProfile g_prof;
+void prof_mark(int stepid, cudaStream_t st) {
+    if (g_prof.on < 0) {
+        const char *e = getenv("QD_PROFILE");
+        g_prof.on = e && atoi(e) > 0;
+    }
+    if (!g_prof.on) return;
+    if (g_prof.used == (int)g_prof.ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        g_prof.ev.push_back(e);
+        g_prof.step.push_back(0);
+    }
+    cudaEventRecord(g_prof.ev[g_prof.used], st);
+    g_prof.step[g_prof.used++] = stepid;
+}
+void prof_collect(cudaStream_t st) {
+    if (g_prof.on <= 0) return;
+    prof_mark(-1, st);
+    cudaStreamSynchronize(st);
+    for (int i = 0; i < 8; i++) g_prof.ms[i] = 0;
+    for (int i = 0; i + 1 < g_prof.used; i++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, g_prof.ev[i], g_prof.ev[i + 1]);
+        if (g_prof.step[i] >= 0) g_prof.ms[g_prof.step[i]] += t;
+    }
+    g_prof.used = 0;
+}
+}  // namespace
+
+// Per-step times (ms) of the last dense->band reduction when QD_PROFILE=1.
+extern "C" int qd_stage1_profile(double *ms, int n) {
+    for (int i = 0; i < n && i < 8; i++) ms[i] = g_prof.ms[i];
+    return QD_OK;
+}
+
 template <typename T>
 static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream_t st) {
     typedef typename Blas<T>::R R;
@@ -342,6 +392,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         T *Rp = (T *)w.Rall + (int64_t)p * b * b;
         T *Pcol = A + k + k * lda;  // rows k.., columns k..k+nb-1
         // 1. bring the panel's b columns up to date with the pending (V, W) terms
+        prof_mark(0, st);
         if (K > 0) {
             BLAS_OK(Blas<T>::gemm(h, N_, C_, (int)(n - k), b, K, &mone, Vacc + off, ldv, Wacc + off, ldv, &one, Pcol,
                                   lda));
@@ -350,9 +401,11 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         }
         // 2. panel QR -> V (explicit, in place), tau, R; nb = min(b, m) reflectors over all b columns
         T *P = A + (k + b) + k * lda;
+        prof_mark(1, st);
         CUDA_OK(cudaMemsetAsync(Rp, 0, sizeof(T) * b * b, st));
         RC(launch_panel<T>(P, lda, m, b, nb, Rp, (T *)w.tau, w, st));
         // 3. T from the Gram matrix
+        prof_mark(2, st);
         BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, m, &one, P, lda, P, lda, &zero, (T *)w.gram, b));
         qd_count_launch(1);
         form_t_kernel<R><<<1, 256, 0, st>>>((const cpx<R> *)w.gram, b, (const cpx<R> *)w.tau, (cpx<R> *)Tp, b, nb);
@@ -362,6 +415,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         T *X = Wacc + (off + b) + (int64_t)K * ldv;
         T *A22 = A + (k + b) + (k + b) * lda;
         BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, nb, &one, P, lda, Tp, b, &zero, VT, m));
+        prof_mark(3, st);
         if (full && w.tc) {
             RC(qd_tc_xprod(A, lda, n, k + b, m, VT, m, nb, X, ldv, w.tc, st));
         } else if (full) {
@@ -371,6 +425,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
                                 (const cuDoubleComplex *)A22, (int)lda, (const cuDoubleComplex *)VT, m,
                                 (const cuDoubleComplex *)&zero, (cuDoubleComplex *)X, (int)ldv));
         }
+        prof_mark(4, st);
         if (K > 0) {
             T *S1 = (T *)w.S1, *S2 = (T *)w.S2;
             BLAS_OK(Blas<T>::gemm(h, C_, N_, K, nb, m, &one, Wacc + off + b, ldv, VT, m, &zero, S1, w.agg));
@@ -379,10 +434,12 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
             BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, K, &mone, Wacc + off + b, ldv, S2, w.agg, &one, X, ldv));
         }
         // 6. W = X - 1/2 V (T^H V^H X)
+        prof_mark(5, st);
         BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, m, &one, P, lda, X, ldv, &zero, (T *)w.M, b));
         BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, nb, &one, Tp, b, (T *)w.M, b, &zero, (T *)w.Y, b));
         BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, nb, &mhalf, P, lda, (T *)w.Y, b, &one, X, ldv));
         // 7. append V (zero above its first row) to Vacc; W already sits in Wacc
+        prof_mark(6, st);
         CUDA_OK(cudaMemset2DAsync(Vacc + (int64_t)K * ldv, sizeof(T) * ldv, 0, sizeof(T) * (off + b), nb, st));
         CUDA_OK(cudaMemset2DAsync(Wacc + (int64_t)K * ldv, sizeof(T) * ldv, 0, sizeof(T) * (off + b), nb, st));
         CUDA_OK(cudaMemcpy2DAsync(Vacc + (off + b) + (int64_t)K * ldv, sizeof(T) * ldv, P, sizeof(T) * lda,
@@ -392,6 +449,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         int64_t kn = k + b;
         bool last = !(kn + b < n);
         if (K + b > w.agg || last) {
+            prof_mark(7, st);
             int mt = (int)(n - kn);
             int64_t offn = kn - k0;
             T *At = A + kn + kn * lda;
@@ -411,6 +469,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
             K = 0;
         }
     }
+    prof_collect(st);
     return QD_OK;
 }
 

@@ -397,6 +397,7 @@ __global__ void dft_axis_kernel(double2 *data, int64_t stride_b, int n0, int n1,
 }
 
 static int dft3(double2 *d, int64_t stride_b, int nb, const Grid3 &g, int sign, cudaStream_t st) {
+    qd_count_launch(3);
     for (int axis = 2; axis >= 0; axis--) {
         int n = g.n[axis];
         int64_t lines = g.size() / n;
@@ -410,6 +411,17 @@ static int dft3(double2 *d, int64_t stride_b, int nb, const Grid3 &g, int sign, 
 }
 
 static inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Batched 3-D DFT (sign -1 forward, +1 inverse without scaling) of nb arrays
+// of n[0] x n[1] x n[2] points, stride_b elements apart; shared with the
+// Coulomb stage.
+extern "C" int qd_dft3_batched(double2 *d, int64_t stride_b, int nb, const int n[3], int sign, void *stream) {
+    Grid3 g = {{n[0], n[1], n[2]}};
+    int rc = dft3(d, stride_b, nb, g, sign, (cudaStream_t)stream);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return QD_OK;
+}
 
 // --------------------------------------------------------------------------
 // Piezoelectric potential (piezo_fourier_coefficient.c:24-132)

@@ -91,8 +91,9 @@ _sig("qd_problem_get_table", ci, [vp, ci, ci, ci, vp, i64])
 _sig("qd_problem_assemble_dev", ci, [vp, vp, i64, ci, ci, vp])
 _sig("qd_eigh_window_dev", ci, [i64, vp, i64, ci, ci, ci, vp, vp, i64, vp])
 _sig("qd_problem_solve", ci, [vp, ci, vp, vp])
-_sig("qd_coulomb", ci, [vp, ci, ci, vp, vp, vp, vp, vp])
+_sig("qd_coulomb", ci, [vp, ci, ci, vp, ci, vp, vp, vp, vp])
 _sig("qd_last_timings", ci, [C.POINTER(C.c_double), ci])
+_sig("qd_stage1_profile", ci, [C.POINTER(C.c_double), ci])
 _sig("qd_tc_work_alloc", ci, [i64, ci, C.POINTER(vp)])
 _sig("qd_tc_work_free", None, [vp])
 _sig("qd_tc_work_check", ci, [vp])
@@ -169,6 +170,12 @@ class Event:
     def __del__(self):
         if self.ev:
             lib.qd_event_destroy(self.ev)
+
+
+def stage1_profile():
+    a = (C.c_double * 8)()
+    lib.qd_stage1_profile(a, 8)
+    return list(a)
 
 
 def last_timings():

@@ -81,6 +81,19 @@ class Problem:
         L.check(L.lib.qd_problem_solve(self._h, prec, w.ctypes.data, v.ctypes.data))
         return w, v
 
+    def coulomb(self, v, n_vb_states, n_cb_states, madelung_ranks=1):
+        """Coulomb matrix elements of the states v (N_H x M, VB states first)
+        with the deck's CME setting (coulomb_matrix_elements.c:24).  Returns
+        the reference's four flat arrays hh, ee, eh_direct, eh_exchange."""
+        nv, nc = n_vb_states, n_cb_states
+        v = np.asfortranarray(v, dtype=np.complex128)
+        out = {"hh": np.zeros(nv ** 4, np.complex128), "ee": np.zeros(nc ** 4, np.complex128),
+               "eh_direct": np.zeros(nv * nv * nc * nc, np.complex128),
+               "eh_exchange": np.zeros(nv * nv * nc * nc, np.complex128)}
+        L.check(L.lib.qd_coulomb(self._h, nv, nc, v.ctypes.data, madelung_ranks, out["hh"].ctypes.data,
+                                 out["ee"].ctypes.data, out["eh_direct"].ctypes.data, out["eh_exchange"].ctypes.data))
+        return out
+
     def energies(self, w, v):
         """Rows of energies_vb.dat (highest state first) and energies_cb.dat
         (write_energies.c:23-93; Bloch characters bloch_character.c:23-105)."""
