@@ -143,7 +143,20 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per launch of xprod_kernel over its algorithmic bytes, from the ncu
+# capture summarised in profiles/xprod_kernel_mg4.txt (one launch, m = 5480).
+XPROD_TRAFFIC_RATIO = 1.086
+
+
+def tc_stats(L, which):
+    import ctypes as C
+    n, ms, work = C.c_longlong(0), C.c_double(0), C.c_double(0)
+    L.check(L.lib.qd_tc_kernel_stats(which, C.byref(n), C.byref(ms), C.byref(work)))
+    return n.value, ms.value, work.value
+
+
 def run_gpu(args, ws, rank, local):
+    import ctypes as C
     import qudos_b200 as q
     from qudos_b200 import configs, lib as L
     if ws > 1:
@@ -155,6 +168,11 @@ def run_gpu(args, ws, rank, local):
         pr.build_tables()
     n, lo, hi = pr.n_h, pr.lo, pr.hi
     M = hi - lo + 1
+    # roofline denominators not in the measured-peak file: cuBLAS TF32 and FP64 GEMM throughput on this GPU
+    tf32_peak, fp64_peak = C.c_double(0), C.c_double(0)
+    L.check(L.lib.qd_gemm_peak(1, 8192, 10, C.byref(tf32_peak)))
+    L.check(L.lib.qd_gemm_peak(0, 8192, 4, C.byref(fp64_peak)))
+    tf32_peak, fp64_peak = tf32_peak.value, fp64_peak.value
     H = L.DeviceBuffer(n * n * 16)
     Z = L.DeviceBuffer(n * M * 16)
     W = L.DeviceBuffer(M * 8)
@@ -181,6 +199,8 @@ def run_gpu(args, ws, rank, local):
     for _ in range(args.warmup):
         step(q.QD_PREC_MIXED)
     launches0 = int(L.lib.qd_launch_count())
+    tc_stats(L, 0)
+    tc_stats(L, 1)  # reset the per-kernel event timers
     barrier(ws)
     L.check(L.lib.qd_device_synchronize())
     with Clocks(local) as clk:
@@ -190,6 +210,8 @@ def run_gpu(args, ws, rank, local):
         e1.record()
         ms = e0.elapsed_ms(e1) / args.steps
     launches = (int(L.lib.qd_launch_count()) - launches0) // args.steps
+    x_n, x_ms, x_bytes = tc_stats(L, 0)
+    f_n, f_ms, f_flops = tc_stats(L, 1)
     ms = allreduce_max(ms, ws)
     tmx = L.last_timings()
     wmx = np.empty(M)
@@ -225,10 +247,25 @@ def run_gpu(args, ws, rank, local):
                             "inverse_iteration": tmx[4], "back_transform": tmx[5], "rayleigh_ritz": tmx[6]},
         "stages_ms_fp64": {"band_reduction": t64[1], "bulge_chasing": t64[2], "bisection": t64[3],
                            "inverse_iteration": t64[4], "back_transform": t64[5]},
-        "roofline": {"bound": "tensor", "kernel": "dense->band reduction (mixed)",
-                     "achieved": flops_stage1 / (st1_ms * 1e-3) / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
-                     "frac": flops_stage1 / (st1_ms * 1e-3) / 1e12 / bf16_peak, "traffic": None,
-                     "note": "16/3 N^3 flop; peak = %s bf16 dense" % peak_src},
+        # the largest kernel with a bandwidth or throughput bound (the bulge chasing ahead of it is latency-bound)
+        "roofline": {"bound": "hbm", "kernel": "xprod_kernel (X = A22 VT, tcgen05 3xTF32)",
+                     "achieved": x_bytes / (x_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": x_bytes / (x_ms * 1e-3) / 1e9 / hbm_peak,
+                     "traffic": XPROD_TRAFFIC_RATIO * x_bytes / max(x_n, 1),
+                     "launches_per_step": x_n / args.steps, "ms_per_step": x_ms / args.steps,
+                     "note": "work = 8 m^2 bytes per launch (trailing matrix read once); peak = %s HBM copy; "
+                             "traffic = dram bytes per launch scaled from one ncu capture" % peak_src},
+        "roofline_flush": {"bound": "tensor", "kernel": "flush_kernel (Hermitian rank-2K update, tcgen05 3xTF32)",
+                           "achieved": f_flops / (f_ms * 1e-3) / 1e12, "peak": tf32_peak / 3.0, "unit": "TFLOP/s",
+                           "frac": f_flops / (f_ms * 1e-3) / 1e12 / (tf32_peak / 3.0), "traffic": None,
+                           "issued_tf32_tflops": 3.0 * f_flops / (f_ms * 1e-3) / 1e12,
+                           "launches_per_step": f_n / args.steps, "ms_per_step": f_ms / args.steps,
+                           "note": "work = 8 mt (mt+1) K flops per launch; peak = measured cuBLAS TF32 GEMM / 3 "
+                                   "(three TF32 products per FP32-accurate product)"},
+        "reduction_fp64_vs_peak": {"achieved": flops_stage1 / (t64[1] * 1e-3) / 1e12, "peak": fp64_peak,
+                                   "unit": "TFLOP/s", "frac": flops_stage1 / (t64[1] * 1e-3) / 1e12 / fp64_peak,
+                                   "note": "FP64 dense->band reduction, 16/3 N^3 flop; peak = measured cuBLAS DGEMM"},
+        "measured_gemm_peaks_tflops": {"tf32": tf32_peak, "fp64": fp64_peak, "bf16": bf16_peak},
         "roofline_assembly": {"bound": "hbm", "achieved": asm_bytes / (ms_asm * 1e-3) / 1e9, "peak": hbm_peak,
                               "unit": "GB/s", "frac": asm_bytes / (ms_asm * 1e-3) / 1e9 / hbm_peak,
                               "traffic": None, "ms": ms_asm},

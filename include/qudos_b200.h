@@ -259,6 +259,19 @@ int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, int m, const
 int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void *V, const void *W, int64_t ldv, int64_t voff,
                 int K, QdTcWork *w, void *stream);
 
+/* Per-kernel device time of the tensor-core building blocks since the last
+ * call (CUDA events around every launch, on the launching stream): which 0
+ * is the X product (work = bytes of the trailing matrix read, 8 m^2 per
+ * launch), 1 the Hermitian rank-2K trailing update (work = 8 mt (mt+1) K
+ * flops per launch).  Synchronises the device and resets the counters. */
+int qd_tc_kernel_stats(int which, long long *launches, double *ms, double *work);
+
+/* Throughput (TFLOP/s) of a plain cuBLAS n^3 GEMM: kind 0 DGEMM (FP64), 1
+ * SGEMM on TF32 tensor cores, 2 ZGEMM; `reps` timed launches after one
+ * warm-up.  Used for the roofline denominators that are not measured
+ * elsewhere. */
+int qd_gemm_peak(int kind, int n, int reps, double *tflops);
+
 /* Allocation-free eigenvalues of a Hermitian tridiagonal matrix for the index
  * window [lo, hi] (0-based, ascending), by the same Sturm-count multisection
  * as the solver's bisection stage.  No reference counterpart: it serves

@@ -600,3 +600,59 @@ extern "C" int qd_stage1_backtransform(const void *A, int64_t n, int64_t lda, in
     if (fp32) return backtransform<cuComplex>((const cuComplex *)A, n, lda, b, w, (cuComplex *)Z, ldz, mz, st);
     return backtransform<cuDoubleComplex>((const cuDoubleComplex *)A, n, lda, b, w, (cuDoubleComplex *)Z, ldz, mz, st);
 }
+
+// Throughput of a plain cuBLAS GEMM (the denominators of the roofline
+// fractions that the measured-peak file does not hold): kind 0 DGEMM (FP64),
+// 1 SGEMM with TF32 tensor-core inputs, 2 ZGEMM.  n x n x n, `reps` timed
+// back-to-back launches after one warm-up; returns TFLOP/s (2 n^3 per real
+// GEMM, 8 n^3 per complex GEMM).
+extern "C" int qd_gemm_peak(int kind, int n, int reps, double *tflops) {
+    if (kind < 0 || kind > 2 || n < 64 || reps < 1) return qd_set_error(QD_ERR_ARG, "qd_gemm_peak: bad arguments");
+    cublasHandle_t h = qd_cublas();
+    if (!h) return qd_set_error(QD_ERR_CUDA, "cuBLAS unavailable");
+    size_t es = kind == 0 ? 8 : kind == 1 ? 4 : 16;
+    void *A = nullptr, *B = nullptr, *C = nullptr;
+    size_t bytes = es * (size_t)n * n;
+    if (cudaMalloc(&A, bytes) != cudaSuccess || cudaMalloc(&B, bytes) != cudaSuccess ||
+        cudaMalloc(&C, bytes) != cudaSuccess) {
+        cudaFree(A);
+        cudaFree(B);
+        cudaGetLastError();
+        return qd_set_error(QD_ERR_NOMEM, "qd_gemm_peak");
+    }
+    cudaMemset(A, 0, bytes);
+    cudaMemset(B, 0, bytes);
+    BLAS_OK(cublasSetStream(h, 0));
+    const double d1 = 1.0, d0 = 0.0;
+    const float f1 = 1.0f, f0 = 0.0f;
+    const cuDoubleComplex z1 = {1, 0}, z0 = {0, 0};
+    auto run = [&]() -> cublasStatus_t {
+        if (kind == 0)
+            return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &d1, (double *)A, n, (double *)B, n, &d0,
+                               (double *)C, n);
+        if (kind == 1)
+            return cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &f1, A, CUDA_R_32F, n, B, CUDA_R_32F, n, &f0, C,
+                                CUDA_R_32F, n, CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
+        return cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &z1, (cuDoubleComplex *)A, n, (cuDoubleComplex *)B, n,
+                           &z0, (cuDoubleComplex *)C, n);
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cublasStatus_t st = run();
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < reps && st == CUBLAS_STATUS_SUCCESS; r++) st = run();
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(A);
+    cudaFree(B);
+    cudaFree(C);
+    if (st != CUBLAS_STATUS_SUCCESS) return qd_set_error(QD_ERR_CUDA, "qd_gemm_peak: cuBLAS status %d", (int)st);
+    double flop = (kind == 2 ? 8.0 : 2.0) * (double)n * n * n * reps;
+    *tflops = flop / (ms * 1e-3) / 1e12;
+    return QD_OK;
+}

@@ -4,10 +4,13 @@
 //    tridiagonal by Householder bulge chasing, eigenvalues only.  Sweep s
 //    annihilates column s below the subdiagonal and chases the bulge down the
 //    band in tasks of b rows.  Sweeps run concurrently in a persistent
-//    cooperative kernel, one sweep per block at a time: task k of sweep s touches
-//    rows/columns [s+1+(k-1)b, s+(k+1)b] and may start once sweep s-1 has
-//    finished its tasks 0..k+2 (the last one overlapping that range).  The wait
-//    on the predecessor's progress counter is bounded.
+//    cooperative kernel.  Task k >= 1 of sweep s reads and writes the block
+//    E = A[s+kb+1 .. s+(k+1)b, s+(k-1)b+1 .. s+kb] and the diagonal block
+//    D = A[s+kb+1 .. s+(k+1)b]^2 (task 0: column s and D = A[s+1 .. s+b]^2).
+//    Task k+1 of sweep s-1 overlaps these (its D shares index s+(k+1)b and its
+//    E the last row of D); task k+2 starts at row s+(k+2)b and column
+//    s+(k+1)b and is disjoint.  So task k may start once sweep s-1 has finished
+//    tasks 0..k+1 (progress counter >= k+2).  The wait is bounded.
 //  * bisect_kernel: eigenvalues of the tridiagonal matrix with indices [lo, hi]
 //    by multisection on Sturm counts (one warp per eigenvalue, 32 shifts per
 //    step).  Selecting by index reproduces zheevr's RANGE='I' window.
@@ -19,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
+#include <string.h>
 
 #include "eig_common.cuh"
 #include "qd_internal.h"
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n,
     for (int s = blockIdx.x; s < n - 1; s += gridDim.x) {
         zd *v = va, *v2 = vb;
         // ---- task 0: annihilate column s below the subdiagonal
-        if (s > 0 && !wait_progress(progress, s - 1, 3, err)) return;
+        if (s > 0 && !wait_progress(progress, s - 1, 2, err)) return;
         int st = s + 1, ed = min(s + b, n - 1), len = ed - st + 1;
         for (int i = t; i < len; i += blockDim.x) v[i] = ldab(AB, ldb, st + i, s);
         for (int idx = t; idx < len * len; idx += blockDim.x) {
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n,
             int J1 = ed + 1;
             if (J1 > n - 1) break;
             int J2 = min(ed + b, n - 1), lm = J2 - J1 + 1;
-            if (s > 0 && !wait_progress(progress, s - 1, k + 3, err)) return;
+            if (s > 0 && !wait_progress(progress, s - 1, k + 2, err)) return;
             // E = A[J1..J2, st..ed] and D = A[J1..J2, J1..J2] in one round trip
             for (int idx = t; idx < lm * len; idx += blockDim.x) {
                 int r = idx % lm, c = idx / lm;
@@ -591,21 +595,21 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
 
 extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *err, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    size_t smem = (size_t)(2 * b * b + 4 * b) * sizeof(zd);
-    CUDA_OK(cudaFuncSetAttribute(hb2st_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev, nsm, per_sm = 0;
     CUDA_OK(cudaGetDevice(&dev));
     CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 256, smem));
-    if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
-    int G = nsm * per_sm;
-    int useful = n / (2 * b) + 2;  // concurrent sweeps are limited by the 3-task lag
-    if (G > useful) G = useful;
-    if (G > n - 1) G = n - 1;
-    if (G < 1) G = 1;
     CUDA_OK(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n, st));
     CUDA_OK(cudaMemsetAsync(err, 0, sizeof(int), st));
     void *args[] = {&AB, &ldb, &n, &b, &progress, &err};
+    size_t smem = (size_t)(2 * b * b + 4 * b) * sizeof(zd);
+    CUDA_OK(cudaFuncSetAttribute(hb2st_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 256, smem));
+    if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
+    int G = nsm * per_sm;
+    int useful = n / (2 * b) + 2;  // concurrent sweeps are limited by the 2-task lag
+    if (G > useful) G = useful;
+    if (G > n - 1) G = n - 1;
+    if (G < 1) G = 1;
     qd_count_launch(1);
     CUDA_OK(cudaLaunchCooperativeKernel((void *)hb2st_kernel, dim3(G), dim3(256), args, smem, st));
     return QD_OK;

@@ -36,6 +36,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <vector>
+
 #include "qd_internal.h"
 
 #define CUDA_OK(x)                                                                                    \
@@ -58,6 +60,7 @@ struct TcArgs {
     int a_x0, a_y0;  // coordinate offsets into the A tensor map
     float2 *C;       // flush: C tile origin; xprod: split-K partials
     int64_t ldc;     // flush: ld of C; xprod: ld of one partial block
+    int kdim;        // flush: rank of the update (K)
     int *err;
 };
 
@@ -101,6 +104,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     }
 }
 
+// Warp-wide bounded wait: lane 0 polls, the warp then synchronises (which
+// orders lane 0's acquire before the other lanes' reads).  All 32 lanes call.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort_flag) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
 __device__ __forceinline__ void tma_load_2d(const CUtensorMap *tm, uint64_t *bar, void *dst, int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
@@ -140,7 +153,7 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t *v) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -149,8 +162,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
           "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
           "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Round to the nearest TF32 value (10 stored mantissa bits, ties away from
 // zero) with integer operations: add half an ulp of TF32 to the magnitude
@@ -206,17 +219,21 @@ __device__ __forceinline__ bool drain_item(float (&acc)[ACC_COLS], int nch, uint
 #pragma unroll
     for (int c = 0; c < ACC_COLS; c++) acc[c] = 0.f;
     for (int ch = 0; ch < nch; ch++) {
-        if (!mbar_wait(&tfull[ab], aphase, abort_flag)) return false;
+        if (!mbar_wait_warp(&tfull[ab], aphase, abort_flag)) return false;
         tc_fence_after();
 #pragma unroll
-        for (int g = 0; g < ACC_COLS / 32; g++) {
-            uint32_t v[32];
-            tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * NCOLS + cbase + g * 32), v);
+        for (int g = 0; g < ACC_COLS / 64; g++) {  // two loads in flight per wait
+            uint32_t v[64];
+            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * NCOLS + cbase + g * 64);
+            tmem_ld32_issue(ta, v);
+            tmem_ld32_issue(ta + 32, v + 32);
+            tmem_ld_wait();
 #pragma unroll
-            for (int c = 0; c < 32; c++) acc[g * 32 + c] += __uint_as_float(v[c]);
+            for (int c = 0; c < 64; c++) acc[g * 64 + c] += __uint_as_float(v[c]);
         }
         tc_fence_before();
-        mbar_arrive(&tempty[ab]);
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(&tempty[ab]);  // one arrival per warp
         if (++ab == 2) {
             ab = 0;
             aphase ^= 1;
@@ -244,18 +261,24 @@ __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
 }
 
 // ---------------------------------------------------------------------------
-// X = A22 VT.  Rings: A (TMA, fp32 -> hi in place) of XA_STAGES x 16 KB, and
-// work slots (lo of A, B hi, B lo) of XW_STAGES x 32 KB.
+// X = A22 VT.  Three rings, each advanced once per k-block:
+//   A  (XA_STAGES x 16 KB): TMA fp32 tiles of A22, turned into hi in place;
+//   B  (XB_STAGES x 16 KB): TMA tiles of the right factor, hi and lo;
+//   L  (XL_STAGES x 16 KB): lo of the A tile, written by the converter.
+// The B tiles come from L2 and have their own producer so that their latency
+// is not serialised behind the converter.
 //   warp 0 A producer, warp 1 MMA, warps 2-5 epilogue, warps 6-9 converter,
 //   warp 10 B producer.
 // ---------------------------------------------------------------------------
-constexpr int XA_STAGES = 7, XW_STAGES = 3;
+constexpr int XA_STAGES = 6, XB_STAGES = 4, XL_STAGES = 3;
 constexpr int X_N = 64;
 constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
-constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB
-constexpr int X_W_BYTES = X_A_BYTES + 2 * X_B_BYTES;
-constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XW_STAGES * X_W_BYTES;
+constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB (hi or lo)
+constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES + XL_STAGES * X_A_BYTES;
 constexpr int X_CHUNK = 2;
+#ifndef X_AGROUP
+#define X_AGROUP 3
+#endif
 constexpr int X_WARPS = 11;
 constexpr int X_TMEM_COLS = 128;
 
@@ -264,13 +287,15 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                  const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint8_t *ringA = smem, *ringW = smem + XA_STAGES * X_A_BYTES;
+    uint8_t *ringA = smem, *ringB = smem + XA_STAGES * X_A_BYTES;
+    uint8_t *ringL = ringB + XB_STAGES * 2 * X_B_BYTES;
     uint64_t *fullA = (uint64_t *)(smem + X_SMEM);
     uint64_t *emptyA = fullA + XA_STAGES;
     uint64_t *fullB = emptyA + XA_STAGES;
-    uint64_t *conv = fullB + XW_STAGES;
-    uint64_t *emptyW = conv + XW_STAGES;
-    uint64_t *tfull = emptyW + XW_STAGES;
+    uint64_t *emptyB = fullB + XB_STAGES;
+    uint64_t *conv = emptyB + XB_STAGES;
+    uint64_t *emptyL = conv + XL_STAGES;
+    uint64_t *tfull = emptyL + XL_STAGES;
     uint64_t *tempty = tfull + 2;
     uint64_t *done = tempty + 2;
     uint32_t *tmem_slot = (uint32_t *)(done + 1);
@@ -282,14 +307,17 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             mbar_init(&fullA[s], 1);
             mbar_init(&emptyA[s], 1);
         }
-        for (int s = 0; s < XW_STAGES; s++) {
+        for (int s = 0; s < XB_STAGES; s++) {
             mbar_init(&fullB[s], 1);
-            mbar_init(&conv[s], 128);
-            mbar_init(&emptyW[s], 1);
+            mbar_init(&emptyB[s], 1);
+        }
+        for (int s = 0; s < XL_STAGES; s++) {
+            mbar_init(&conv[s], 4);  // one arrival per converter warp
+            mbar_init(&emptyL[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 128);
+            mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
         mbar_init(done, 1);
         *abort_flag = 0;
@@ -311,10 +339,11 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
     };
 
     if (warp == 0 || warp == 10) {
-        // ---------------- producers: A ring (warp 0), B into work slots (warp 10) ----------------
+        // ---------------- producers: A ring (warp 0), B ring (warp 10) ----------------
         if (lane == 0) {
             const bool isA = warp == 0;
-            const int nst = isA ? XA_STAGES : XW_STAGES;
+            const int nst = isA ? XA_STAGES : XB_STAGES;
+            uint64_t *full = isA ? fullA : fullB, *empty = isA ? emptyA : emptyB;
             int s = 0;
             uint32_t ph = 0;
             long issued = 0;
@@ -323,20 +352,35 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                 int tm, sp, kb0, kb1;
                 xprod_item(args, item, tm, sp, kb0, kb1);
                 for (int kb = kb0; kb < kb1; kb++) {
-                    if (!mbar_wait(isA ? &emptyA[s] : &emptyW[s], ph ^ 1, abort_flag)) {
+                    // A tiles go out in groups of X_AGROUP adjacent k-blocks (their
+                    // slots are waited for first), so each column of A22 is fetched
+                    // in runs of X_AGROUP * 128 bytes rather than 128-byte pieces.
+                    if (isA && (kb - kb0) % X_AGROUP == 0) {
+                        int s2 = s;
+                        uint32_t ph2 = ph;
+                        for (int g = 1; g < X_AGROUP && kb + g < kb1 && ok; g++) {
+                            ring_next(s2, ph2, nst);
+                            if (!mbar_wait(&empty[s2], ph2 ^ 1, abort_flag)) {
+                                fail(1);
+                                ok = false;
+                            }
+                        }
+                        if (!ok) break;
+                    }
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) {
                         fail(isA ? 1 : 6);
                         ok = false;
                         break;
                     }
                     if (isA) {
-                        mbar_expect_tx(&fullA[s], X_A_BYTES);
-                        tma_load_2d(&tmA, &fullA[s], ringA + s * X_A_BYTES, args.a_x0 + kb * BKF,
+                        mbar_expect_tx(&full[s], X_A_BYTES);
+                        tma_load_2d(&tmA, &full[s], ringA + s * X_A_BYTES, args.a_x0 + kb * BKF,
                                     args.a_y0 + tm * TILE_M);
                     } else {
-                        uint8_t *w = ringW + s * X_W_BYTES;
-                        mbar_expect_tx(&fullB[s], 2 * X_B_BYTES);
-                        tma_load_2d(&tmB, &fullB[s], w + X_A_BYTES, kb * BKF, 0);
-                        tma_load_2d(&tmBlo, &fullB[s], w + X_A_BYTES + X_B_BYTES, kb * BKF, 0);
+                        uint8_t *b = ringB + s * 2 * X_B_BYTES;
+                        mbar_expect_tx(&full[s], 2 * X_B_BYTES);
+                        tma_load_2d(&tmB, &full[s], b, kb * BKF, 0);
+                        tma_load_2d(&tmBlo, &full[s], b + X_B_BYTES, kb * BKF, 0);
                     }
                     issued++;
                     ring_next(s, ph, nst);
@@ -345,15 +389,15 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             long outstanding = issued < nst ? issued : nst;
             for (long q = 0; q < outstanding; q++) {
                 ring_prev(s, ph, nst);
-                wait_bounded(isA ? &fullA[s] : &fullB[s], ph);
+                wait_bounded(&full[s], ph);
             }
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer (accumulation restarted every X_CHUNK k-blocks) ----------------
         if (lane == 0) {
             const uint32_t idesc = tf32_idesc(TILE_M, X_N);
-            int sa = 0, sw = 0, ab = 0;
-            uint32_t pa = 0, pw = 0, aphase = 0;
+            int sa = 0, sb = 0, sl = 0, ab = 0;
+            uint32_t pa = 0, pb = 0, pl = 0, aphase = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
                 int tm, sp, kb0, kb1;
@@ -368,7 +412,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         }
                         tc_fence_after();
                     }
-                    if (!mbar_wait(&fullB[sw], pw, abort_flag) || !mbar_wait(&conv[sw], pw, abort_flag)) {
+                    if (!mbar_wait(&fullB[sb], pb, abort_flag) || !mbar_wait(&conv[sl], pl, abort_flag)) {
                         fail(3);
                         ok = false;
                         break;
@@ -376,8 +420,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     tc_fence_after();
                     const uint32_t d = tmem_base + (uint32_t)(ab * X_N);
                     const uint32_t a_hi = smem_u32(ringA + sa * X_A_BYTES);
-                    const uint32_t a_lo = smem_u32(ringW + sw * X_W_BYTES);
-                    const uint32_t b_hi = a_lo + X_A_BYTES, b_lo = b_hi + X_B_BYTES;
+                    const uint32_t a_lo = smem_u32(ringL + sl * X_A_BYTES);
+                    const uint32_t b_hi = smem_u32(ringB + sb * 2 * X_B_BYTES), b_lo = b_hi + X_B_BYTES;
 #pragma unroll
                     for (int kk = 0; kk < BKF / 8; kk++) {
                         uint32_t o = kk * 32;
@@ -387,9 +431,11 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
                     }
                     umma_commit(&emptyA[sa]);
-                    umma_commit(&emptyW[sw]);
+                    umma_commit(&emptyB[sb]);
+                    umma_commit(&emptyL[sl]);
                     ring_next(sa, pa, XA_STAGES);
-                    ring_next(sw, pw, XW_STAGES);
+                    ring_next(sb, pb, XB_STAGES);
+                    ring_next(sl, pl, XL_STAGES);
                     if (cpos == X_CHUNK - 1 || kb == kb1 - 1) {
                         umma_commit(&tfull[ab]);
                         if (++ab == 2) {
@@ -424,22 +470,22 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             }
         }
     } else {
-        // ---------------- converter: A fp32 -> hi (in place) + lo (work slot) ----------------
+        // ---------------- converter: A fp32 -> hi (in place) + lo (L ring) ----------------
         const int t = threadIdx.x - 6 * 32;  // 0..127
-        int sa = 0, sw = 0;
-        uint32_t pa = 0, pw = 0;
+        int sa = 0, sl = 0;
+        uint32_t pa = 0, pl = 0;
         bool ok = true;
         for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
             int tm, sp, kb0, kb1;
             xprod_item(args, item, tm, sp, kb0, kb1);
             for (int kb = kb0; kb < kb1; kb++) {
-                if (!mbar_wait(&fullA[sa], pa, abort_flag) || !mbar_wait(&emptyW[sw], pw ^ 1, abort_flag)) {
+                if (!mbar_wait_warp(&fullA[sa], pa, abort_flag) || !mbar_wait_warp(&emptyL[sl], pl ^ 1, abort_flag)) {
                     fail(5);
                     ok = false;
                     break;
                 }
                 float4 *a = (float4 *)(ringA + sa * X_A_BYTES);
-                float4 *alo = (float4 *)(ringW + sw * X_W_BYTES);
+                float4 *alo = (float4 *)(ringL + sl * X_A_BYTES);
 #pragma unroll
                 for (int u = 0; u < X_A_BYTES / 16 / 128; u++) {
                     int idx = u * 128 + t;
@@ -452,9 +498,10 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     alo[idx] = l;
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(&conv[sw]);
+                __syncwarp();
+                if ((threadIdx.x & 31) == 0) mbar_arrive(&conv[sl]);  // one arrival per warp
                 ring_next(sa, pa, XA_STAGES);
-                ring_next(sw, pw, XW_STAGES);
+                ring_next(sl, pl, XL_STAGES);
             }
         }
     }
@@ -506,7 +553,7 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 256);
+            mbar_init(&tempty[b], 8);  // one arrival per epilogue warp
         }
         mbar_init(done, 1);
         *abort_flag = 0;
@@ -768,7 +815,27 @@ int sm_count() {
     return g_nsm;
 }
 
-constexpr int SMEM_EXTRA = 1024 /*alignment*/ + 256 /*barriers*/;
+constexpr int SMEM_EXTRA = 1024 /*alignment*/ + 512 /*barriers*/;
+
+// Device time of every launch of the two kernels, bracketed by CUDA events on
+// the launching stream; read (and reset) by qd_tc_kernel_stats.  Also the
+// algorithmic work of each launch: bytes of the trailing matrix read by the
+// X product (8 m^2), flops of the Hermitian rank-2K update (8 mt (mt+1) K).
+struct KernelTimer {
+    std::vector<cudaEvent_t> ev;
+    int used = 0;
+    double work = 0.0;
+};
+KernelTimer g_timer[2];
+void timer_mark(int which, cudaStream_t st) {
+    KernelTimer &t = g_timer[which];
+    if (t.used == (int)t.ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        t.ev.push_back(e);
+    }
+    cudaEventRecord(t.ev[t.used++], st);
+}
 
 int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &blo, const TcArgs &args,
                  cudaStream_t st) {
@@ -781,8 +848,11 @@ int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &
     int grid = args.n_items < sm_count() ? args.n_items : sm_count();
     if (grid < 1) return QD_OK;
     qd_count_launch(1);
+    timer_mark(0, st);
     xprod_kernel<<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
     CUDA_OK(cudaGetLastError());
+    timer_mark(0, st);
+    g_timer[0].work += 8.0 * (double)args.rows * (double)args.rows;
     return QD_OK;
 }
 
@@ -797,8 +867,11 @@ int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap
     int grid = args.n_items < sm_count() ? args.n_items : sm_count();
     if (grid < 1) return QD_OK;
     qd_count_launch(1);
+    timer_mark(1, st);
     flush_kernel<<<grid, F_WARPS * 32, smem, st>>>(a, alo, b, blo, args);
     CUDA_OK(cudaGetLastError());
+    timer_mark(1, st);
+    g_timer[1].work += 8.0 * (double)args.rows * (double)(args.rows + 1) * (double)args.kdim;
     return QD_OK;
 }
 
@@ -903,6 +976,7 @@ extern "C" int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, i
     if (splits < 1) splits = 1;
     a.splits = splits;
     a.n_items = a.tiles_m * splits;
+    a.kdim = 0;
     a.rows = m;
     a.cols = nb;
     a.a_x0 = (int)(2 * off);
@@ -944,6 +1018,7 @@ extern "C" int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void
     a.splits = 1;
     a.kblocks = (int)((pitch + BKF - 1) / BKF);
     a.n_items = a.tiles_m * (a.tiles_m + 1) / 2;  // lower-triangle tiles
+    a.kdim = K;
     a.rows = mt;
     a.cols = mt;
     a.a_x0 = 0;
@@ -952,4 +1027,25 @@ extern "C" int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void
     a.ldc = lda;
     a.err = w->err;
     return launch_flush(ta, talo, tb, tblo, a, st);
+}
+
+// Launches, summed device time (ms) and algorithmic work of the X-product
+// (which = 0; work in bytes) or trailing-update kernel (which = 1; work in
+// flops) since the previous call; synchronises the device.
+extern "C" int qd_tc_kernel_stats(int which, long long *launches, double *ms, double *work) {
+    if (which < 0 || which > 1) return qd_set_error(QD_ERR_ARG, "qd_tc_kernel_stats: which must be 0 or 1");
+    CUDA_OK(cudaDeviceSynchronize());
+    KernelTimer &t = g_timer[which];
+    double total = 0.0;
+    for (int i = 0; i + 1 < t.used; i += 2) {
+        float x = 0.f;
+        CUDA_OK(cudaEventElapsedTime(&x, t.ev[i], t.ev[i + 1]));
+        total += x;
+    }
+    *launches = t.used / 2;
+    *ms = total;
+    *work = t.work;
+    t.used = 0;
+    t.work = 0.0;
+    return QD_OK;
 }

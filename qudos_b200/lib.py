@@ -99,6 +99,8 @@ _sig("qd_tc_work_free", None, [vp])
 _sig("qd_tc_work_check", ci, [vp])
 _sig("qd_tc_xprod", ci, [vp, i64, i64, i64, ci, vp, i64, ci, vp, i64, vp, vp])
 _sig("qd_tc_flush", ci, [vp, i64, i64, ci, vp, vp, i64, i64, ci, vp, vp])
+_sig("qd_tc_kernel_stats", ci, [ci, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)])
+_sig("qd_gemm_peak", ci, [ci, ci, ci, C.POINTER(C.c_double)])
 _sig("qd_tridiag_eigvals_noalloc", ci, [vp, ci, ci, ci, ci, vp, vp])
 _sig("qd_tridiag_bisect", ci, [vp, ci, ci, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_dev_alloc", ci, [C.c_size_t, C.POINTER(vp)])
