@@ -262,23 +262,22 @@ __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
 
 // ---------------------------------------------------------------------------
 // X = A22 VT.  Three rings, each advanced once per k-block:
-//   A  (XA_STAGES x 16 KB): TMA fp32 tiles of A22, turned into hi in place;
+//   A  (XA_STAGES x 16 KB): TMA fp32 tiles of A22, released as soon as the
+//      converter has read them, so that the ring turns over at DRAM latency;
 //   B  (XB_STAGES x 16 KB): TMA tiles of the right factor, hi and lo;
-//   L  (XL_STAGES x 16 KB): lo of the A tile, written by the converter.
+//   L  (XL_STAGES x 32 KB): hi and lo of the A tile, written by the converter
+//      and read by the MMAs.
 // The B tiles come from L2 and have their own producer so that their latency
 // is not serialised behind the converter.
 //   warp 0 A producer, warp 1 MMA, warps 2-5 epilogue, warps 6-9 converter,
 //   warp 10 B producer.
 // ---------------------------------------------------------------------------
-constexpr int XA_STAGES = 6, XB_STAGES = 4, XL_STAGES = 3;
+constexpr int XA_STAGES = 6, XB_STAGES = 3, XL_STAGES = 2;
 constexpr int X_N = 64;
 constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
 constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB (hi or lo)
-constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES + XL_STAGES * X_A_BYTES;
+constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES + XL_STAGES * 2 * X_A_BYTES;
 constexpr int X_CHUNK = 2;
-#ifndef X_AGROUP
-#define X_AGROUP 3
-#endif
 constexpr int X_WARPS = 11;
 constexpr int X_TMEM_COLS = 128;
 
@@ -305,7 +304,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < XA_STAGES; s++) {
             mbar_init(&fullA[s], 1);
-            mbar_init(&emptyA[s], 1);
+            mbar_init(&emptyA[s], 4);  // released by the four converter warps
         }
         for (int s = 0; s < XB_STAGES; s++) {
             mbar_init(&fullB[s], 1);
@@ -352,21 +351,6 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                 int tm, sp, kb0, kb1;
                 xprod_item(args, item, tm, sp, kb0, kb1);
                 for (int kb = kb0; kb < kb1; kb++) {
-                    // A tiles go out in groups of X_AGROUP adjacent k-blocks (their
-                    // slots are waited for first), so each column of A22 is fetched
-                    // in runs of X_AGROUP * 128 bytes rather than 128-byte pieces.
-                    if (isA && (kb - kb0) % X_AGROUP == 0) {
-                        int s2 = s;
-                        uint32_t ph2 = ph;
-                        for (int g = 1; g < X_AGROUP && kb + g < kb1 && ok; g++) {
-                            ring_next(s2, ph2, nst);
-                            if (!mbar_wait(&empty[s2], ph2 ^ 1, abort_flag)) {
-                                fail(1);
-                                ok = false;
-                            }
-                        }
-                        if (!ok) break;
-                    }
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) {
                         fail(isA ? 1 : 6);
                         ok = false;
@@ -396,8 +380,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         // ---------------- MMA issuer (accumulation restarted every X_CHUNK k-blocks) ----------------
         if (lane == 0) {
             const uint32_t idesc = tf32_idesc(TILE_M, X_N);
-            int sa = 0, sb = 0, sl = 0, ab = 0;
-            uint32_t pa = 0, pb = 0, pl = 0, aphase = 0;
+            int sb = 0, sl = 0, ab = 0;
+            uint32_t pb = 0, pl = 0, aphase = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
                 int tm, sp, kb0, kb1;
@@ -419,8 +403,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     }
                     tc_fence_after();
                     const uint32_t d = tmem_base + (uint32_t)(ab * X_N);
-                    const uint32_t a_hi = smem_u32(ringA + sa * X_A_BYTES);
-                    const uint32_t a_lo = smem_u32(ringL + sl * X_A_BYTES);
+                    const uint32_t a_hi = smem_u32(ringL + sl * 2 * X_A_BYTES);
+                    const uint32_t a_lo = a_hi + X_A_BYTES;
                     const uint32_t b_hi = smem_u32(ringB + sb * 2 * X_B_BYTES), b_lo = b_hi + X_B_BYTES;
 #pragma unroll
                     for (int kk = 0; kk < BKF / 8; kk++) {
@@ -430,10 +414,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_lo + o), idesc, 1u);
                         umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
                     }
-                    umma_commit(&emptyA[sa]);
                     umma_commit(&emptyB[sb]);
                     umma_commit(&emptyL[sl]);
-                    ring_next(sa, pa, XA_STAGES);
                     ring_next(sb, pb, XB_STAGES);
                     ring_next(sl, pl, XL_STAGES);
                     if (cpos == X_CHUNK - 1 || kb == kb1 - 1) {
@@ -470,7 +452,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             }
         }
     } else {
-        // ---------------- converter: A fp32 -> hi (in place) + lo (L ring) ----------------
+        // ---------------- converter: A fp32 -> hi and lo (L ring); releases the A slot ----------------
         const int t = threadIdx.x - 6 * 32;  // 0..127
         int sa = 0, sl = 0;
         uint32_t pa = 0, pl = 0;
@@ -484,8 +466,9 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     ok = false;
                     break;
                 }
-                float4 *a = (float4 *)(ringA + sa * X_A_BYTES);
-                float4 *alo = (float4 *)(ringL + sl * X_A_BYTES);
+                const float4 *a = (const float4 *)(ringA + sa * X_A_BYTES);
+                float4 *ahi = (float4 *)(ringL + sl * 2 * X_A_BYTES);
+                float4 *alo = (float4 *)(ringL + sl * 2 * X_A_BYTES + X_A_BYTES);
 #pragma unroll
                 for (int u = 0; u < X_A_BYTES / 16 / 128; u++) {
                     int idx = u * 128 + t;
@@ -494,12 +477,15 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     split3(x.y, h.y, l.y);
                     split3(x.z, h.z, l.z);
                     split3(x.w, h.w, l.w);
-                    a[idx] = h;
+                    ahi[idx] = h;
                     alo[idx] = l;
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if ((threadIdx.x & 31) == 0) mbar_arrive(&conv[sl]);  // one arrival per warp
+                if ((threadIdx.x & 31) == 0) {  // one arrival per warp
+                    mbar_arrive(&emptyA[sa]);
+                    mbar_arrive(&conv[sl]);
+                }
                 ring_next(sa, pa, XA_STAGES);
                 ring_next(sl, pl, XL_STAGES);
             }
@@ -528,6 +514,9 @@ constexpr int F_B_BYTES = F_N * BKF * 4;     // 32 KB
 constexpr int F_STAGE_BYTES = 2 * F_A_BYTES + 2 * F_B_BYTES;
 constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES;
 constexpr int F_EPI_COLS = 128;
+#ifndef F_CHUNK
+#define F_CHUNK 2  // k-blocks per accumulation chunk
+#endif
 constexpr int F_WARPS = 10;
 constexpr int F_TMEM_COLS = 512;
 
@@ -613,8 +602,14 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
             uint32_t ph = 0, aphase = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < args.n_items && ok; item += gridDim.x) {
-                for (int kb = 0; kb < args.kblocks; kb++) {  // one k-block per accumulation chunk
-                    if (!mbar_wait(&tempty[ab], aphase ^ 1, abort_flag) || !mbar_wait(&full[s], ph, abort_flag)) {
+                for (int kb = 0; kb < args.kblocks; kb++) {  // F_CHUNK k-blocks per accumulation chunk
+                    const int cpos = kb % F_CHUNK;
+                    if (cpos == 0 && !mbar_wait(&tempty[ab], aphase ^ 1, abort_flag)) {
+                        fail(2);
+                        ok = false;
+                        break;
+                    }
+                    if (!mbar_wait(&full[s], ph, abort_flag)) {
                         fail(3);
                         ok = false;
                         break;
@@ -626,16 +621,18 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
 #pragma unroll
                     for (int kk = 0; kk < BKF / 8; kk++) {
                         uint32_t o = kk * 32;
-                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_hi + o), idesc, kk > 0 ? 1u : 0u);
+                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_hi + o), idesc, (cpos > 0 || kk > 0) ? 1u : 0u);
                         umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_lo + o), idesc, 1u);
                         umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
                     }
                     umma_commit(&empty[s]);
-                    umma_commit(&tfull[ab]);
                     ring_next(s, ph, F_STAGES);
-                    if (++ab == 2) {
-                        ab = 0;
-                        aphase ^= 1;
+                    if (cpos == F_CHUNK - 1 || kb == args.kblocks - 1) {
+                        umma_commit(&tfull[ab]);
+                        if (++ab == 2) {
+                            ab = 0;
+                            aphase ^= 1;
+                        }
                     }
                 }
             }
@@ -651,7 +648,7 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
             int tm, tn;
             lower_tile(item, T, tm, tn);
             float acc[F_EPI_COLS];
-            if (!drain_item<F_N, F_EPI_COLS>(acc, args.kblocks, tmem_base, q, cbase, ab, aphase, tfull, tempty,
+            if (!drain_item<F_N, F_EPI_COLS>(acc, (args.kblocks + F_CHUNK - 1) / F_CHUNK, tmem_base, q, cbase, ab, aphase, tfull, tempty,
                                              abort_flag)) {
                 fail(4);
                 break;
