@@ -241,6 +241,33 @@ int qd_last_timings(double *ms, int n);
  * [7] trailing rank-2K updates.  Adds one event per step boundary. */
 int qd_stage1_profile(double *ms, int n);
 
+/* Hellmann-Feynman gradients dE_n/dp = <psi_n| dH/dp |psi_n> of the states in
+ * eigvec_host (N_H x n_states, host, normalised eigenvectors of the problem's
+ * H) with respect to the parameters in params:
+ *   QD_GRAD_LENGTH       Length `index` (1..5) of shape `shape`   per nm
+ *   QD_GRAD_BASE         Lengths 1 and 2 of shape `shape` together per nm
+ *   QD_GRAD_COMPOSITION  composition x of shape `shape`           per unit x
+ *   QD_GRAD_FIELD        field component `index` (0 x, 1 y, 2 z)  per kV/cm
+ *   QD_GRAD_EP           relative scale of the binary-table Ep     per unit scale
+ *   QD_GRAD_GAMMA1       relative scale of the binary-table gamma_1 per unit scale
+ * H is linear in the per-difference coefficient tables, so dH/dp is the
+ * Hamiltonian of dcoef/dp; that table derivative is a central difference of
+ * the coefficient tables (step rel_step times the parameter's magnitude, with
+ * a floor; rel_step <= 0 selects 1e-4), and the contraction with the states
+ * runs on the GPU without materialising dH.  No counterpart in the reference.
+ * dEdp[k * n_states + n] receives the derivative of state n for parameter k. */
+enum {
+    QD_GRAD_LENGTH = 0,
+    QD_GRAD_BASE = 1,
+    QD_GRAD_COMPOSITION = 2,
+    QD_GRAD_FIELD = 3,
+    QD_GRAD_EP = 4,
+    QD_GRAD_GAMMA1 = 5
+};
+typedef struct { int kind, shape, index; } qd_grad_param;
+int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int n_states,
+                           const qd_grad_param *params, int n_params, double rel_step, double *dEdp);
+
 /* Tensor-core building blocks of the mixed-precision reduction (tcgen05
  * kind::tf32 with a 3xTF32 hi/lo split, FP32 accumulation), exposed for
  * tests.  All pointers are device pointers to column-major complex64 data.

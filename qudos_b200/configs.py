@@ -62,11 +62,14 @@ def lens_7(mg=3):
     return params, cell
 
 
-def pyramid_11(mg=5, n_states=8, cme=1):
+def pyramid_11(mg=5, n_states=8, cme=1, height=5.0, half_base=9.0, x=0.4, fz=10.0):
+    """The truncated-pyramid deck; height, half_base (nm), the dot's composition
+    x (1 - In fraction) and Fz (kV/cm) are the parameters the gradients are
+    taken with respect to."""
     params = parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg, M_S_Gy=mg, M_S_Gz=mg, N_VB=n_states,
-                             N_CB=n_states, Piezo=1, Fz=10, CME=cme, M_C_Gx=mg, M_C_Gy=mg, M_C_Gz=mg)
+                             N_CB=n_states, Piezo=1, Fz=fz, CME=cme, M_C_Gx=mg, M_C_Gy=mg, M_C_Gz=mg)
     cell = (supercell_record((36.0, 36.0, 24.0)) +
-            shape_record(6, 3, 0.4, 0.0, (0.0, 0.0, -2.5), (9.0, 9.0, 4.0, 5.0)) +
+            shape_record(6, 3, x, 0.0, (0.0, 0.0, -2.5), (half_base, half_base, 4.0, height)) +
             shape_record(17, 3, 0.4, 0.0, (0.0, 0.0, -2.8), (2.0, 0.6)))
     return params, cell
 

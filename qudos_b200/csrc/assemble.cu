@@ -223,3 +223,132 @@ extern "C" int qd_assemble_dual_launch(const void *d_coef, const double *d_Gx, c
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
     return QD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Hellmann-Feynman contraction: g_s = psi_s^H dH psi_s for the states of a
+// window, where dH is the Hamiltonian built from a derivative coefficient
+// table.  H is linear in the coefficient table (every element is a sum of
+// table entries times polynomials in G, G' and K), so dH/dp is the same
+// polynomial evaluated on d(coef)/dp; its elements are generated on the fly
+// and contracted at once with all states, never stored.  Lower-triangle
+// elements count twice (dH is Hermitian): g = sum_{r>c} 2 Re(conj(psi_r) dH_rc
+// psi_c) + sum_r dH_rr |psi_r|^2.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int GRAD_MB = 16;  // states per pass (held in registers per row)
+
+__global__ void __launch_bounds__(128) grad_contract_kernel(Ctx c, int64_t npw, int64_t nh, const double2 *psi,
+                                                            int64_t ldz, int m, int cols_per, double *partial) {
+    __shared__ double red[GRAD_MB][4];
+    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t col0 = (int64_t)blockIdx.y * cols_per;
+    const int64_t block = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    double acc[GRAD_MB];
+#pragma unroll
+    for (int s = 0; s < GRAD_MB; s++) acc[s] = 0.0;
+    const int64_t row_first = blockIdx.x * (int64_t)blockDim.x;
+    const bool skip = row_first + blockDim.x - 1 < col0;  // tile entirely above the diagonal
+    if (!skip && row < nh) {
+        zc pr[GRAD_MB];
+#pragma unroll
+        for (int s = 0; s < GRAD_MB; s++)
+            pr[s] = s < m ? conj(zc(psi[row + s * ldz])) : zc(0.0);
+        const int rb = (int)(row / npw);
+        const int i = (int)(row - rb * npw);
+        const int r[3] = {i / (c.N[1] * c.N[2]), (i / c.N[2]) % c.N[1], i % c.N[2]};
+        const int64_t col_end = col0 + cols_per < nh ? col0 + cols_per : nh;
+        for (int64_t col = col0; col < col_end && col <= row; col++) {
+            const int cb = (int)(col / npw);
+            const int j = (int)(col - cb * npw);
+            const int q[3] = {j / (c.N[1] * c.N[2]), (j / c.N[2]) % c.N[1], j % c.N[2]};
+            zc v = band_element(c, rb, cb, r, q);
+            if (col < row) v = 2.0 * v;
+#pragma unroll
+            for (int s = 0; s < GRAD_MB; s++) {
+                if (s < m) {
+                    zc t = pr[s] * v * zc(psi[col + s * ldz]);
+                    acc[s] += t.re;
+                }
+            }
+        }
+    }
+    // block reduction per state
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < GRAD_MB; s++) {
+        double x = acc[s];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[s][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < GRAD_MB)
+        partial[block * GRAD_MB + threadIdx.x] =
+            red[threadIdx.x][0] + red[threadIdx.x][1] + red[threadIdx.x][2] + red[threadIdx.x][3];
+}
+
+__global__ void grad_sum_kernel(const double *partial, int64_t nblocks, double *out) {
+    __shared__ double red[32];
+    const int s = blockIdx.x;
+    double x = 0.0;
+    for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x) x += partial[b * GRAD_MB + s];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+        out[s] = t;
+    }
+}
+
+// d = (plus - minus) * scale, element-wise over n complex values
+__global__ void coef_diff_kernel(const double2 *plus, const double2 *minus, int64_t n, double scale, double2 *d) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        d[t] = make_double2((plus[t].x - minus[t].x) * scale, (plus[t].y - minus[t].y) * scale);
+}
+}  // namespace
+
+extern "C" int qd_coef_diff(const void *plus, const void *minus, int64_t n, double scale, void *d, void *stream) {
+    qd_count_launch(1);
+    coef_diff_kernel<<<1024, 256, 0, (cudaStream_t)stream>>>((const double2 *)plus, (const double2 *)minus, n, scale,
+                                                             (double2 *)d);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "coef diff: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
+// out[s] = psi_s^H dH psi_s for s < m (device pointers; psi column-major N_H x m, ld ldz).
+extern "C" int qd_grad_contract(const void *d_dcoef, const double *d_Gx, const double *d_Gy, const double *d_Gz,
+                                const int N[3], const double K[3], const void *psi, int64_t ldz, int m,
+                                double *out_dev, void *stream) {
+    if (upload_block_map() != QD_OK) return qd_set_error(QD_ERR_CUDA, "block map upload failed");
+    Ctx c;
+    c.coef = (const double2 *)d_dcoef;
+    c.G[0] = d_Gx; c.G[1] = d_Gy; c.G[2] = d_Gz;
+    for (int a = 0; a < 3; a++) {
+        c.N[a] = N[a];
+        c.NT[a] = 2 * N[a] - 1;
+        c.off[a] = c.NT[a] / 2 - N[a] / 2;
+        c.K[a] = K[a];
+    }
+    c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
+    const int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
+    const int cols_per = 64;
+    dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
+    const int64_t nblocks = (int64_t)grid.x * grid.y;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *partial = nullptr;
+    if (qd_pool_alloc((void **)&partial, sizeof(double) * (size_t)nblocks * GRAD_MB, st))
+        return qd_set_error(QD_ERR_NOMEM, "gradient partial sums");
+    for (int s0 = 0; s0 < m; s0 += GRAD_MB) {
+        int mb = m - s0 < GRAD_MB ? m - s0 : GRAD_MB;
+        qd_count_launch(2);
+        grad_contract_kernel<<<grid, 128, 0, st>>>(c, npw, nh, (const double2 *)psi + s0 * ldz, ldz, mb, cols_per,
+                                                   partial);
+        grad_sum_kernel<<<mb, 256, 0, st>>>(partial, nblocks, out_dev + s0);
+    }
+    cudaError_t e = cudaGetLastError();
+    qd_pool_free(partial, st);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "gradient contraction: %s", cudaGetErrorString(e));
+    return QD_OK;
+}

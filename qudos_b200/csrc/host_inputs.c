@@ -329,11 +329,20 @@ static double interp(int bowing, int type, double x, double y, const double P[4]
            y * (1.0 - x - y) * B[2];
 }
 
+/* Scale factors applied to the Ep and Luttinger gamma_1 columns of the binary
+ * table before interpolation (1 = the table as published); the gradient
+ * entry point differentiates with respect to them. */
+double qd_scale_Ep = 1.0, qd_scale_gL1 = 1.0;
+
 int qd_material_parameters(double T, int include_piezo, int n_shape, struct supercell_geometry *geo,
                            struct material_params *out) {
     double col[QD_N_BINARY_COLS][QD_N_BINARY];
     for (int i = 0; i < QD_N_BINARY; i++)
         for (int c = 0; c < QD_N_BINARY_COLS; c++) col[c][i] = qd_binary_rows[i][c];
+    for (int i = 0; i < QD_N_BINARY; i++) {
+        col[C_Ep][i] *= qd_scale_Ep;
+        col[C_gL1][i] *= qd_scale_gL1;
+    }
     for (int s = 0; s < n_shape; s++) {
         if (geo[s].material < 0 || geo[s].material > 14)
             return qd_set_error(QD_ERR_INPUT, "Requested material system not recognised");

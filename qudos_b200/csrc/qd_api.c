@@ -563,3 +563,162 @@ void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coul
                              struct supercell_geometry *supercell, struct material_params *parameters, int *N_states,
                              struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb,
                              struct coulomb_matrix_element CME, int coulomb_region_type);
+
+/* ------------------------------------------------------------------------- */
+/* Hellmann-Feynman gradients of the window's eigenvalues                     */
+/* ------------------------------------------------------------------------- */
+int qd_coef_diff(const void *plus, const void *minus, int64_t n, double scale, void *d, void *stream);
+int qd_grad_contract(const void *d_dcoef, const double *d_Gx, const double *d_Gy, const double *d_Gz, const int N[3],
+                     const double K[3], const void *psi, int64_t ldz, int m, double *out_dev, void *stream);
+
+/* Every device table of the problem is freed (the next build allocates anew). */
+static void release_tables(qd_problem *pr) {
+    for (int a = 0; a < 3; a++) {
+        if (pr->d_G[a]) cudaFree(pr->d_G[a]);
+        if (pr->d_GS[a]) cudaFree(pr->d_GS[a]);
+        pr->d_G[a] = NULL;
+        pr->d_GS[a] = NULL;
+    }
+    void **dev[] = {&pr->d_geo, &pr->d_mat, &pr->d_chi_s, &pr->d_eps_s, &pr->d_phi_s, &pr->d_chi,
+                    &pr->d_eps, &pr->d_phi, &pr->d_conv, &pr->d_coef};
+    for (size_t i = 0; i < sizeof(dev) / sizeof(dev[0]); i++) {
+        if (*dev[i]) cudaFree(*dev[i]);
+        *dev[i] = NULL;
+    }
+    pr->tables_ready = 0;
+}
+
+static double *grad_length(struct supercell_geometry *g, int k) {
+    switch (k) {
+        case 1: return &g->L1;
+        case 2: return &g->L2;
+        case 3: return &g->L3;
+        case 4: return &g->L4;
+        case 5: return &g->L5;
+        default: return NULL;
+    }
+}
+
+/* Apply value offset `delta` (internal units) to parameter q; materials are
+ * re-evaluated.  Returns the parameter's current value through *value. */
+static int grad_apply(qd_problem *pr, const qd_grad_param *q, double delta, double *value) {
+    struct supercell_geometry *g = NULL;
+    if (q->kind <= QD_GRAD_COMPOSITION) {
+        if (q->shape < 1 || q->shape >= pr->p.n_shape)
+            return qd_set_error(QD_ERR_ARG, "gradient parameter: shape index %d out of range", q->shape);
+        g = &pr->geo[q->shape];
+    }
+    double *x = NULL;
+    switch (q->kind) {
+        case QD_GRAD_LENGTH:
+            x = grad_length(g, q->index);
+            if (!x) return qd_set_error(QD_ERR_ARG, "gradient parameter: length index %d not in 1..5", q->index);
+            break;
+        case QD_GRAD_BASE:
+            g->L2 += delta;
+            x = &g->L1;
+            break;
+        case QD_GRAD_COMPOSITION: x = &g->x; break;
+        case QD_GRAD_FIELD:
+            if (q->index < 0 || q->index > 2) return qd_set_error(QD_ERR_ARG, "field component %d", q->index);
+            x = &pr->p.F[q->index];
+            break;
+        case QD_GRAD_EP: x = &qd_scale_Ep; break;
+        case QD_GRAD_GAMMA1: x = &qd_scale_gL1; break;
+        default: return qd_set_error(QD_ERR_ARG, "gradient parameter kind %d", q->kind);
+    }
+    *x += delta;
+    if (value) *value = *x;
+    return qd_material_parameters(pr->p.T, pr->p.piezo, pr->p.n_shape, pr->geo, pr->mat);
+}
+
+/* Step floor (internal units) and the factor from the internal derivative to
+ * the reported one (per nm, per unit composition, per kV/cm, per unit scale). */
+static void grad_units(int kind, double *floor_, double *to_user) {
+    switch (kind) {
+        case QD_GRAD_LENGTH:
+        case QD_GRAD_BASE: *floor_ = 10.0; *to_user = 10.0; break;        /* Angstrom -> per nm */
+        case QD_GRAD_COMPOSITION: *floor_ = 0.1; *to_user = 1.0; break;
+        case QD_GRAD_FIELD: *floor_ = 1.0e-5; *to_user = 1.0e-5; break;   /* V/Angstrom -> per kV/cm */
+        default: *floor_ = 1.0; *to_user = 1.0; break;                     /* relative scales */
+    }
+}
+
+int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int n_states,
+                           const qd_grad_param *params, int n_params, double rel_step, double *dEdp) {
+    if (!pr || !eigvec_host || !params || !dEdp || n_states < 1 || n_params < 1)
+        return qd_set_error(QD_ERR_ARG, "eigen_gradients_8_band: bad arguments");
+    if (!(rel_step > 0.0)) rel_step = 1e-4;
+    RC(qd_problem_build_tables(pr));
+    const int64_t nt = pr->nT, ncoef = (int64_t)QD_N_COEF * nt, nh = pr->n_h;
+    void *Z = NULL, *dplus = NULL, *dminus = NULL, *dcoef = NULL;
+    double *out = NULL;
+    int rc = QD_OK;
+    if (qd_pool_alloc(&Z, sizeof(qd_complex128) * (size_t)nh * n_states, NULL) ||
+        qd_pool_alloc(&dplus, sizeof(qd_complex128) * (size_t)ncoef, NULL) ||
+        qd_pool_alloc(&dminus, sizeof(qd_complex128) * (size_t)ncoef, NULL) ||
+        qd_pool_alloc(&dcoef, sizeof(qd_complex128) * (size_t)ncoef, NULL) ||
+        qd_pool_alloc((void **)&out, sizeof(double) * (size_t)n_params * n_states, NULL))
+        rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band: work buffers");
+    if (rc == QD_OK && cudaMemcpy(Z, eigvec_host, sizeof(qd_complex128) * (size_t)nh * n_states,
+                                  cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: eigenvector upload");
+    /* originals, restored exactly after each parameter */
+    const int ns = pr->p.n_shape;
+    struct supercell_geometry *geo0 = (struct supercell_geometry *)malloc(sizeof(*geo0) * ns);
+    qd_params p0 = pr->p;
+    const double sEp = qd_scale_Ep, sg1 = qd_scale_gL1;
+    if (!geo0) rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band");
+    else memcpy(geo0, pr->geo, sizeof(*geo0) * ns);
+    for (int k = 0; rc == QD_OK && k < n_params; k++) {
+        const qd_grad_param *q = &params[k];
+        double v0 = 0.0, floor_ = 1.0, to_user = 1.0;
+        if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
+        grad_units(q->kind, &floor_, &to_user);
+        const double h = rel_step * (fabs(v0) > floor_ ? fabs(v0) : floor_);
+        for (int side = 0; rc == QD_OK && side < 2; side++) {
+            double dummy;
+            if ((rc = grad_apply(pr, q, side == 0 ? h : -h, &dummy))) break;
+            release_tables(pr);
+            if ((rc = qd_tables_build_dev(pr))) break;
+            if (cudaMemcpy(side == 0 ? dplus : dminus, pr->d_coef, sizeof(qd_complex128) * (size_t)ncoef,
+                           cudaMemcpyDeviceToDevice) != cudaSuccess)
+                rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: table copy");
+            /* back to the exact original values before the other side */
+            memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
+            pr->p = p0;
+            qd_scale_Ep = sEp;
+            qd_scale_gL1 = sg1;
+            if (rc == QD_OK) rc = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+        }
+        if (rc) break;
+        if ((rc = qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL))) break;
+        rc = qd_grad_contract(dcoef, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, Z, nh, n_states,
+                              out + (size_t)k * n_states, NULL);
+    }
+    /* the problem's own tables again */
+    if (geo0) {
+        memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
+        free(geo0);
+    }
+    pr->p = p0;
+    qd_scale_Ep = sEp;
+    qd_scale_gL1 = sg1;
+    int rc2 = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+    release_tables(pr);
+    if (rc2 == QD_OK) rc2 = qd_tables_build_dev(pr);
+    if (rc == QD_OK) rc = rc2;
+    if (rc == QD_OK) {
+        if (cudaMemcpy(dEdp, out, sizeof(double) * (size_t)n_params * n_states, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: copy-out");
+        for (int k = 0; rc == QD_OK && k < n_params; k++) {
+            double floor_, to_user;
+            grad_units(params[k].kind, &floor_, &to_user);
+            for (int s = 0; s < n_states; s++) dEdp[(size_t)k * n_states + s] *= to_user;
+        }
+    }
+    void *bufs[] = {Z, dplus, dminus, dcoef, out};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        if (bufs[i]) qd_pool_free(bufs[i], NULL);
+    return rc;
+}

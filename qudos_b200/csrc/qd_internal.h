@@ -52,6 +52,7 @@ int qd_read_supercell_text(const char *text, const qd_params *p, struct supercel
 int qd_material_parameters(double T, int include_piezo, int n_shape, struct supercell_geometry *geo,
                            struct material_params *out);
 void qd_basis_grid(int n_T, double L, double *out);
+extern double qd_scale_Ep, qd_scale_gL1;
 
 void qd_count_launch(int n);
 

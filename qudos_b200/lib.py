@@ -94,6 +94,12 @@ _sig("qd_problem_solve", ci, [vp, ci, vp, vp])
 _sig("qd_coulomb", ci, [vp, ci, ci, vp, ci, vp, vp, vp, vp])
 _sig("qd_last_timings", ci, [C.POINTER(C.c_double), ci])
 _sig("qd_stage1_profile", ci, [C.POINTER(C.c_double), ci])
+class GradParam(C.Structure):
+    _fields_ = [("kind", ci), ("shape", ci), ("index", ci)]
+
+
+QD_GRAD_LENGTH, QD_GRAD_BASE, QD_GRAD_COMPOSITION, QD_GRAD_FIELD, QD_GRAD_EP, QD_GRAD_GAMMA1 = range(6)
+_sig("eigen_gradients_8_band", ci, [vp, vp, ci, C.POINTER(GradParam), ci, C.c_double, vp])
 _sig("qd_tc_work_alloc", ci, [i64, ci, C.POINTER(vp)])
 _sig("qd_tc_work_free", None, [vp])
 _sig("qd_tc_work_check", ci, [vp])

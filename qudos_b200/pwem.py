@@ -94,6 +94,19 @@ class Problem:
                                  out["ee"].ctypes.data, out["eh_direct"].ctypes.data, out["eh_exchange"].ctypes.data))
         return out
 
+    def gradients(self, v, params, rel_step=1e-4):
+        """Hellmann-Feynman derivatives <psi_n| dH/dp |psi_n> of the states v
+        (N_H x M) for params = [(kind, shape, index), ...] (lib.QD_GRAD_*).
+        Returns (len(params), M): per nm, per unit composition, per kV/cm or per
+        unit relative scale."""
+        v = np.asfortranarray(v, dtype=np.complex128)
+        m = v.shape[1]
+        arr = (L.GradParam * len(params))(*[L.GradParam(*p) for p in params])
+        out = np.zeros((len(params), m))
+        L.check(L.lib.eigen_gradients_8_band(self._h, v.ctypes.data, m, arr, len(params), rel_step,
+                                             out.ctypes.data))
+        return out
+
     def energies(self, w, v):
         """Rows of energies_vb.dat (highest state first) and energies_cb.dat
         (write_energies.c:23-93; Bloch characters bloch_character.c:23-105)."""
