@@ -241,6 +241,15 @@ int qd_last_timings(double *ms, int n);
  * [7] trailing rank-2K updates.  Adds one event per step boundary. */
 int qd_stage1_profile(double *ms, int n);
 
+/* Batched solves of independent problems (no counterpart in the reference):
+ * problems[k] is solved as by qd_problem_solve(problems[k], prec, eigval[k],
+ * eigvec[k]) (host outputs of M_k and N_H,k x M_k values).  Up to n_threads
+ * solves run at once, each from its own host thread on its own stream,
+ * largest instances first, so that small latency-bound solves overlap on the
+ * GPU.  Returns the first failure. */
+int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, double *const *eigval,
+                        qd_complex128 *const *eigvec);
+
 /* Hellmann-Feynman gradients dE_n/dp = <psi_n| dH/dp |psi_n> of the states in
  * eigvec_host (N_H x n_states, host, normalised eigenvectors of the problem's
  * H) with respect to the parameters in params:

@@ -7,7 +7,7 @@ cores) is the one the process uses.
 
 from . import lib  # noqa: F401  (loads libqdgpu.so; raises if it is missing)
 from .lib import QD_PREC_FP64, QD_PREC_MIXED, QDError, device_count  # noqa: F401
-from .pwem import Problem, eigh_window_dev, write_energies  # noqa: F401
+from .pwem import Problem, eigh_window_dev, solve_batch, write_energies  # noqa: F401
 
-__all__ = ["Problem", "QDError", "QD_PREC_FP64", "QD_PREC_MIXED", "device_count", "eigh_window_dev",
+__all__ = ["Problem", "QDError", "QD_PREC_FP64", "QD_PREC_MIXED", "device_count", "solve_batch", "eigh_window_dev",
            "write_energies"]

@@ -2,7 +2,9 @@
 
     python qudos_b200/build.py
 
-nvcc cross-compiles for sm_100a without a GPU.  cuBLAS is linked from the CUDA
+nvcc cross-compiles for sm_100a without a GPU.  Everything is built with the
+per-thread default stream, so that solves driven from several host threads
+(the batched entry point) overlap instead of serialising on one stream.  cuBLAS is linked from the CUDA
 toolkit (12.9) with an RPATH to it; the CUDA runtime is linked statically.
 """
 
@@ -19,7 +21,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["tables.cu", "assemble.cu", "eig_stage1.cu", "eig_stage2.cu", "eig_driver.cu", "coulomb.cu", "tc_gemm.cu"]
-C_SOURCES = ["host_inputs.c", "qd_api.c"]
+C_SOURCES = ["host_inputs.c", "qd_api.c", "batch.c"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -47,7 +49,7 @@ def build(verbose=False, force=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
         if force or _stale(o, [s] + headers):
-            cmd = [NVCC, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
+            cmd = [NVCC, "-std=c++17", "-O3", "-lineinfo", "--default-stream", "per-thread", *ARCH, "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
                    "-c", s, "-o", o]
             out = _run(cmd)
             if verbose:
@@ -57,7 +59,7 @@ def build(verbose=False, force=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
         if force or _stale(o, [s] + headers):
-            _run(["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-I" + os.path.join(ROOT, "include"),
+            _run(["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-DCUDA_API_PER_THREAD_DEFAULT_STREAM=1", "-I" + os.path.join(ROOT, "include"),
                   "-I" + os.path.join(CUDA, "include"), "-c", s, "-o", o])
         objs.append(o)
     if force or _stale(OUT, objs):

@@ -83,6 +83,32 @@ def molecule_15(mg=7, n_states=8):
     return params, cell
 
 
+def batch_lenses(n=64, seed=0):
+    """The batched sweep: n lens dots (In(c)Ga(1-c)As on a 0.5 nm wetting layer of
+    the same alloy, in a 40 x 40 x 24 nm GaAs cell) with radius U[8, 14] nm,
+    height U[2, 5] nm, In fraction c U[0.4, 1.0], Fz U[-50, 50] kV/cm and a
+    plane-wave cutoff drawn from {7^3, 9^3, 11^3}, in that draw order per
+    instance from numpy.random.default_rng(seed); 4 e + 4 h Kramers pairs each.
+    Returns a list of (params, cell, description)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        r = rng.uniform(8.0, 14.0)
+        h = rng.uniform(2.0, 5.0)
+        c = rng.uniform(0.4, 1.0)
+        fz = rng.uniform(-50.0, 50.0)
+        mg = int(rng.integers(3, 6))
+        x = 1.0 - c
+        params = parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg, M_S_Gy=mg, M_S_Gz=mg, N_VB=4,
+                                 N_CB=4, Piezo=1, Fz=fz)
+        cell = (supercell_record((40.0, 40.0, 24.0)) +
+                shape_record(4, 3, x, 0.0, (0.0, 0.0, -0.5 * h), (r, r, h)) +
+                shape_record(17, 3, x, 0.0, (0.0, 0.0, -0.5 * h - 0.25), (2.0, 0.5)))
+        out.append((params, cell, dict(radius=r, height=h, indium=c, fz=fz, mg=mg)))
+    return out
+
+
 DECKS = {"lens_7": lens_7, "pyramid_11": pyramid_11, "molecule_15": molecule_15}
 
 

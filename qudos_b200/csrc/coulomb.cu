@@ -399,7 +399,7 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
         return qd_set_error(QD_ERR_CUDA, "cuBLAS unavailable");
     }
     const cuDoubleComplex one = {1, 0}, zero = {0, 0};
-    cublasStatus_t bs = cublasSetStream(h, st);
+    cublasStatus_t bs = cublasSetStream(h, st ? st : cudaStreamPerThread);
     if (bs == CUBLAS_STATUS_SUCCESS)
         bs = cublasZgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, P, P, (int)SC, &one, (const cuDoubleComplex *)Brw, (int)SC,
                          (const cuDoubleComplex *)BC, (int)SC, &zero, (cuDoubleComplex *)U, P);

@@ -38,7 +38,7 @@ extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const do
                              double2 *Z, int64_t ldz, double bnorm, double2 *ywork, void *stream);
 extern "C" cublasHandle_t qd_cublas(void);
 
-static double g_timings[8];
+static thread_local double g_timings[8];  // per host thread (concurrent batched solves)
 extern "C" int qd_last_timings(double *ms, int n) {
     for (int i = 0; i < n && i < 8; i++) ms[i] = g_timings[i];
     return QD_OK;
@@ -421,7 +421,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         tm.mark();  // 5
         // ---- FP64 Rayleigh-Ritz against H (lower triangle, complex128)
         cublasHandle_t h = qd_cublas();
-        BLAS_OK(cublasSetStream(h, st));
+        BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
         double2 *Y, *S, *Ak, *C, *Xn;
         double *theta;
         int *info;

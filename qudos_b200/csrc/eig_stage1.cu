@@ -336,7 +336,7 @@ struct StageProfile {
     int used = 0;
     double ms[8] = {0};
 };
-StageProfile g_prof;
+thread_local StageProfile g_prof;
 void prof_mark(int stepid, cudaStream_t st) {
     if (g_prof.on < 0) {
         const char *e = getenv("QD_PROFILE");
@@ -377,7 +377,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
     typedef typename Blas<T>::R R;
     const bool full = sizeof(R) == 4;
     cublasHandle_t h = qd_cublas();
-    BLAS_OK(cublasSetStream(h, st));
+    BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
     const T one = cval<T>(1, 0), zero = cval<T>(0, 0), mone = cval<T>(-1, 0), mhalf = cval<T>(-0.5, 0);
     const cublasOperation_t N_ = CUBLAS_OP_N, C_ = CUBLAS_OP_C;
     T *Vacc = (T *)w.Vacc, *Wacc = (T *)w.Wacc;
@@ -578,7 +578,7 @@ template <typename T>
 static int backtransform(const T *A, int64_t n, int64_t lda, int b, const Stage1Work *w, T *Z, int64_t ldz, int mz,
                          cudaStream_t st) {
     cublasHandle_t h = qd_cublas();
-    BLAS_OK(cublasSetStream(h, st));
+    BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
     const T one = cval<T>(1, 0), zero = cval<T>(0, 0), mone = cval<T>(-1, 0);
     for (int p = w->npanels - 1; p >= 0; p--) {
         int64_t k = (int64_t)p * b;
@@ -622,7 +622,7 @@ extern "C" int qd_gemm_peak(int kind, int n, int reps, double *tflops) {
     }
     cudaMemset(A, 0, bytes);
     cudaMemset(B, 0, bytes);
-    BLAS_OK(cublasSetStream(h, 0));
+    BLAS_OK(cublasSetStream(h, cudaStreamPerThread));
     const double d1 = 1.0, d0 = 0.0;
     const float f1 = 1.0f, f0 = 0.0f;
     const cuDoubleComplex z1 = {1, 0}, z0 = {0, 0};

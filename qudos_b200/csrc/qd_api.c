@@ -178,7 +178,9 @@ int qd_event_destroy(void *ev) {
         if (rc_ != QD_OK) return rc_; \
     } while (0)
 
-static cublasHandle_t g_cublas = NULL;
+/* one handle per host thread: concurrent solves on several threads each drive
+ * their own per-thread default stream */
+static __thread cublasHandle_t g_cublas = NULL;
 cublasHandle_t qd_cublas(void) {
     if (!g_cublas) {
         cublasCreate(&g_cublas);
@@ -188,15 +190,15 @@ cublasHandle_t qd_cublas(void) {
         typedef cublasStatus_t (*set_strategy_fn)(cublasHandle_t, int);
         set_strategy_fn f = (set_strategy_fn)dlsym(RTLD_DEFAULT, "cublasSetEmulationStrategy");
         if (f) f(g_cublas, 2 /* CUBLAS_EMULATION_STRATEGY_EAGER */);
+        cublasSetStream(g_cublas, cudaStreamPerThread);
     }
     return g_cublas;
 }
 
-/* complex64 GEMM arithmetic of the mixed path: 2 = FP32 emulated with BF16x9 on
- * the tensor cores (default), 1 = TF32, 0 = plain FP32.  QD_MIXED_GEMM overrides. */
+/* complex64 GEMM arithmetic of the mixed path: 3 = the library's tcgen05
+ * 3xTF32 kernels (default); 2, 1, 0 = cuBLAS CGEMM with FP32 emulated by BF16x9,
+ * with TF32, or in plain FP32 (for comparison).  QD_MIXED_GEMM overrides. */
 int qd_mixed_gemm_mode(void) {
-    /* 3: the library's tcgen05 3xTF32 kernels; 0-2: cuBLAS CGEMM (FP32 SIMT,
-     * TF32, BF16x9 emulation) for comparison */
     const char *s = getenv("QD_MIXED_GEMM");
     return s ? atoi(s) : 3;
 }

@@ -823,7 +823,7 @@ struct KernelTimer {
     int used = 0;
     double work = 0.0;
 };
-KernelTimer g_timer[2];
+thread_local KernelTimer g_timer[2];
 void timer_mark(int which, cudaStream_t st) {
     KernelTimer &t = g_timer[which];
     if (t.used == (int)t.ev.size()) {

@@ -99,6 +99,7 @@ class GradParam(C.Structure):
 
 
 QD_GRAD_LENGTH, QD_GRAD_BASE, QD_GRAD_COMPOSITION, QD_GRAD_FIELD, QD_GRAD_EP, QD_GRAD_GAMMA1 = range(6)
+_sig("eigenstates_batched", ci, [C.POINTER(vp), ci, ci, ci, C.POINTER(vp), C.POINTER(vp)])
 _sig("eigen_gradients_8_band", ci, [vp, vp, ci, C.POINTER(GradParam), ci, C.c_double, vp])
 _sig("qd_tc_work_alloc", ci, [i64, ci, C.POINTER(vp)])
 _sig("qd_tc_work_free", None, [vp])

@@ -118,6 +118,18 @@ class Problem:
         return rows[:m_vb][::-1], rows[m_vb:]
 
 
+def solve_batch(problems, prec=L.QD_PREC_MIXED, n_threads=8):
+    """Solve independent problems concurrently (eigenstates_batched).  Returns a
+    list of (eigval[M], eigvec N_H x M) in the order of `problems`."""
+    outs = [(np.empty(p.m), np.empty((p.n_h, p.m), dtype=np.complex128, order="F")) for p in problems]
+    n = len(problems)
+    hs = (C.c_void_p * n)(*[p.handle.value for p in problems])
+    ws = (C.c_void_p * n)(*[o[0].ctypes.data for o in outs])
+    vs = (C.c_void_p * n)(*[o[1].ctypes.data for o in outs])
+    L.check(L.lib.eigenstates_batched(hs, n, prec, n_threads, ws, vs))
+    return outs
+
+
 def eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream=None):
     L.check(L.lib.qd_eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream))
 
