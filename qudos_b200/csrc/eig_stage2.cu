@@ -33,65 +33,6 @@ typedef cpx<double> zd;
 #define PROGRESS_DONE 0x7fffffff
 #define QD_INVIT_ITERS 2
 
-// ---------------------------------------------------------------------------
-// Householder helpers in shared memory (one warp computes, results broadcast)
-// ---------------------------------------------------------------------------
-// x[0..len) -> v (v[0] = 1), returns beta (real) and tau; zlarfg conventions.
-__device__ void larfg_warp(zd *x, int len, double *beta_out, zd *tau_out) {
-    int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int i = 1 + lane; i < len; i += 32) s += cabs2(x[i]);
-    s = warp_sum(s);
-    zd alpha = x[0];
-    double beta;
-    zd tau, scale;
-    if (s == 0.0 && alpha.im == 0.0) {
-        beta = alpha.re;
-        tau = mk<double>(0, 0);
-        scale = mk<double>(0, 0);
-    } else {
-        beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + s), alpha.re);
-        tau = mk<double>((beta - alpha.re) / beta, -alpha.im / beta);
-        double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
-        scale = mk<double>(dr / den, -di / den);
-    }
-    __syncwarp();
-    for (int i = 1 + lane; i < len; i += 32) x[i] = cmul(x[i], scale);
-    if (lane == 0) x[0] = mk<double>(1, 0);
-    __syncwarp();
-    *beta_out = beta;
-    *tau_out = tau;
-}
-
-// D (n x n full Hermitian, ld) <- H^H D H, H = I - tau v v^H.
-__device__ void sym_update(zd *D, int ld, int n, const zd *v, zd tau, zd *w, double *scratch) {
-    // w = tau D v
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        zd acc = mk<double>(0, 0);
-        for (int c = 0; c < n; c++) acc = cadd(acc, cmul(D[r + c * ld], v[c]));
-        w[r] = cmul(tau, acc);
-    }
-    __syncthreads();
-    // c = Re(conj(tau) v^H w) ... (real for Hermitian D)
-    double part = 0.0;
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        zd t = cmulc(v[r], w[r]);   // conj(v) w
-        zd ct = cmulc(tau, t);      // conj(tau) * t
-        part += ct.re;
-    }
-    double cc = block_sum(part, scratch);
-    for (int r = threadIdx.x; r < n; r += blockDim.x) w[r] = csub(w[r], mk<double>(0.5 * cc * v[r].re, 0.5 * cc * v[r].im));
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        int r = idx % n, c = idx / n;
-        // D -= v w^H + w v^H
-        zd a = cmul(v[r], cconj(w[c]));
-        zd b = cmul(w[r], cconj(v[c]));
-        D[r + c * ld] = csub(D[r + c * ld], cadd(a, b));
-    }
-    __syncthreads();
-}
-
 __device__ __forceinline__ zd ldab(const double2 *AB, int ldb, int64_t i, int64_t j) {  // i >= j
     double2 v = __ldcg(&AB[(i - j) + j * (int64_t)ldb]);
     return mk<double>(v.x, v.y);
@@ -127,94 +68,121 @@ __device__ bool wait_progress(const int *progress, int s_prev, int need, int *er
     return ok != 0;
 }
 
+// The block barrier orders every thread's stores before thread 0's release
+// store (release at gpu scope is cumulative over what thread 0 has observed).
 __device__ __forceinline__ void publish(int *progress, int s, int val) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(progress + s, val);
+    if (threadIdx.x == 0) st_release(progress + s, val);
+}
+
+// ---------------------------------------------------------------------------
+// Warp-register helpers for the bulge chasing.  Blocks are at most 32 x 32;
+// lane r holds row r, warp w holds the columns w + 8 i (i = 0..3).
+// ---------------------------------------------------------------------------
+#define HB_NW 8  // warps per block
+#define HB_NC 4  // columns per thread (32 / HB_NW)
+
+__device__ __forceinline__ zd shfl_z(zd a, int src) {
+    return mk<double>(__shfl_sync(0xffffffffu, a.re, src), __shfl_sync(0xffffffffu, a.im, src));
+}
+__device__ __forceinline__ zd warp_sum_z(zd a) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a.re += __shfl_xor_sync(0xffffffffu, a.re, o);
+        a.im += __shfl_xor_sync(0xffffffffu, a.im, o);
+    }
+    return a;
+}
+
+// Householder reflector of the warp-distributed vector x (lane r holds x[r],
+// zero for r >= len), zlarfg conventions: H^H x = beta e_0 with
+// H = I - tau v v^H, v[0] = 1.  Every lane returns its v[r]; beta and tau are
+// the same in all lanes.
+__device__ __forceinline__ zd larfg_lanes(zd x, int len, double *beta_out, zd *tau_out) {
+    const int r = threadIdx.x & 31;
+    double s = warp_sum(r >= 1 && r < len ? cabs2(x) : 0.0);
+    zd alpha = shfl_z(x, 0);
+    double beta;
+    zd tau, scale;
+    if (s == 0.0 && alpha.im == 0.0) {
+        beta = alpha.re;
+        tau = mk<double>(0, 0);
+        scale = mk<double>(0, 0);
+    } else {
+        beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + s), alpha.re);
+        tau = mk<double>((beta - alpha.re) / beta, -alpha.im / beta);
+        double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
+        scale = mk<double>(dr / den, -di / den);
+    }
+    *beta_out = beta;
+    *tau_out = tau;
+    if (r == 0) return mk<double>(1, 0);
+    return r < len ? cmul(x, scale) : mk<double>(0, 0);
+}
+
+// Loads the Hermitian diagonal block D = A[r0 .. r0+len-1]^2 from the lower band.
+__device__ __forceinline__ void load_diag_block(zd (&D)[HB_NC], const double2 *AB, int ldb, int64_t r0, int len) {
+    const int r = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < HB_NC; i++) {
+        int c = w + HB_NW * i;
+        D[i] = mk<double>(0, 0);
+        if (r < len && c < len) D[i] = r >= c ? ldab(AB, ldb, r0 + r, r0 + c) : cconj(ldab(AB, ldb, r0 + c, r0 + r));
     }
 }
 
-// 8 threads per output: out[o] = sum_i M(o, i) * x[i] (complex), n_out <= 32, n_in <= 32.
-// mode 0: out[r] = sum_c E[r + c*ld] x[c]; mode 1: out[c] = sum_r conj(x[r]) E[r + c*ld].
-// Every lane of the warp must call it (the reduction shuffles over all 32 lanes);
-// lanes whose output index is out of range pass valid = false.
-__device__ __forceinline__ zd dot8(const zd *E, int ld, const zd *x, int o, int n_in, int part, int mode, bool valid) {
-    zd acc = mk<double>(0, 0);
-    for (int i = part; valid && i < n_in; i += 8) {
-        if (mode == 0) acc = cadd(acc, cmul(E[o + i * ld], x[i]));
-        else acc = cadd(acc, cmulc(x[i], E[i + o * ld]));
-    }
-    for (int off = 4; off > 0; off >>= 1) {
-        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, off);
-        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, off);
-    }
-    return acc;
-}
-
-// c = Re(conj(tau) v^H u) for vectors of length n <= 32, computed by a whole warp.
-__device__ __forceinline__ double warp_vhu(const zd *v, const zd *u, zd tau, int n) {
-    int lane = threadIdx.x & 31;
-    double part = 0.0;
-    if (lane < n) part = cmulc(tau, cmulc(v[lane], u[lane])).re;
-    return warp_sum(part);
-}
-
-// Two-sided update of the Hermitian block D (n x n, ld b) with H = I - tau v v^H,
-// given u = tau D v: D <- D - v u'^H - u' v^H, u' = u - 1/2 c v, c = Re(conj(tau) v^H u).
-// Writes the lower triangle to the band at (r0, r0).
-__device__ __forceinline__ void sym_apply_store(zd *D, int ldD, int n, const zd *v, const zd *u, zd tau, double2 *AB,
-                                                int ldb, int64_t r0) {
-    double c = warp_vhu(v, u, tau, n);
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        int r = idx % n, q = idx / n;
-        if (r < q) continue;
-        zd ur = csub(u[r], mk<double>(0.5 * c * v[r].re, 0.5 * c * v[r].im));
-        zd uq = csub(u[q], mk<double>(0.5 * c * v[q].re, 0.5 * c * v[q].im));
-        zd val = csub(D[r + q * ldD], cadd(cmul(v[r], cconj(uq)), cmul(ur, cconj(v[q]))));
-        if (r == q) val.im = 0.0;
-        stab(AB, ldb, r0 + r, r0 + q, val);
+// Two-sided update D <- H^H D H with H = I - tau v v^H, given the partial sums
+// of D v over this warp's columns; stores the lower triangle at (r0, r0).
+// part: HB_NW x 32 shared scratch.  vr = v[r], vc[i] = v[w + 8 i].
+__device__ __forceinline__ void diag_update_store(const zd (&D)[HB_NC], zd dv_part, zd vr, const zd (&vc)[HB_NC],
+                                                  zd tau, int len, zd (*part)[32], double2 *AB, int ldb, int64_t r0) {
+    const int r = threadIdx.x & 31, w = threadIdx.x >> 5;
+    part[w][r] = dv_part;
+    __syncthreads();
+    zd u = mk<double>(0, 0);
+#pragma unroll
+    for (int q = 0; q < HB_NW; q++) u = cadd(u, part[q][r]);
+    u = cmul(tau, u);  // u = tau D v
+    double c = warp_sum(cmulc(tau, cmulc(vr, u)).re);  // Re(conj(tau) v^H u)
+    u = csub(u, mk<double>(0.5 * c * vr.re, 0.5 * c * vr.im));
+#pragma unroll
+    for (int i = 0; i < HB_NC; i++) {
+        int col = w + HB_NW * i;
+        zd uc = shfl_z(u, col);
+        zd val = csub(D[i], cadd(cmul(vr, cconj(uc)), cmul(u, cconj(vc[i]))));
+        if (r == col) val.im = 0.0;
+        if (r < len && col < len && r >= col) stab(AB, ldb, r0 + r, r0 + col, val);
     }
 }
 
-__global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n, int b, int *progress, int *err) {
-    extern __shared__ unsigned char sm_raw[];
-    zd *D = (zd *)sm_raw;        // b x b
-    zd *E = D + b * b;           // b x b
-    zd *va = E + b * b;          // b : current reflector
-    zd *vb = va + b;             // b : next reflector
-    zd *u = vb + b;              // b
-    zd *w = u + b;               // b
-    __shared__ double s_beta;
-    __shared__ zd s_tau;
-    const int t = threadIdx.x, part = t & 7, o8 = t >> 3;
+// Bulge chasing, one sweep per block at a time.  Task 0 of sweep s annihilates
+// column s below the subdiagonal: v from A[s+1 .., s], then the two-sided update
+// of D = A[s+1 .. s+b]^2.  Task k >= 1 applies the previous reflector to
+// E = A[J1 .. J2, st .. ed] from the right, annihilates E[:, 0] below its first
+// row with a new reflector applied from the left to E and two-sided to
+// D = A[J1 .. J2]^2.  E and D live in registers; every warp forms the reflector
+// itself from its own copy of the first column, so a task has two block
+// barriers (the row sums E v and D v cross the warps).
+__global__ void __launch_bounds__(256, 3) hb2st_kernel(double2 *AB, int ldb, int n, int b, int *progress, int *err) {
+    __shared__ zd partA[HB_NW][32];
+    __shared__ zd partB[HB_NW][32];
+    const int r = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int s = blockIdx.x; s < n - 1; s += gridDim.x) {
-        zd *v = va, *v2 = vb;
-        // ---- task 0: annihilate column s below the subdiagonal
         if (s > 0 && !wait_progress(progress, s - 1, 2, err)) return;
         int st = s + 1, ed = min(s + b, n - 1), len = ed - st + 1;
-        for (int i = t; i < len; i += blockDim.x) v[i] = ldab(AB, ldb, st + i, s);
-        for (int idx = t; idx < len * len; idx += blockDim.x) {
-            int r = idx % len, c = idx / len;
-            D[r + c * b] = r >= c ? ldab(AB, ldb, st + r, st + c) : cconj(ldab(AB, ldb, st + c, st + r));
+        zd D[HB_NC], E[HB_NC], vc[HB_NC];
+        zd x = r < len ? ldab(AB, ldb, st + r, s) : mk<double>(0, 0);
+        load_diag_block(D, AB, ldb, st, len);
+        double beta;
+        zd tau;
+        zd vr = larfg_lanes(x, len, &beta, &tau);
+        if (w == 0 && r < len) stab(AB, ldb, st + r, s, r == 0 ? mk<double>(beta, 0.0) : mk<double>(0, 0));
+        zd dv = mk<double>(0, 0);
+#pragma unroll
+        for (int i = 0; i < HB_NC; i++) {
+            vc[i] = shfl_z(vr, w + HB_NW * i);
+            dv = cadd(dv, cmul(D[i], vc[i]));
         }
-        __syncthreads();
-        if (t < 32) {
-            double beta;
-            zd tau;
-            larfg_warp(v, len, &beta, &tau);
-            if (t == 0) { s_beta = beta; s_tau = tau; }
-        }
-        __syncthreads();
-        zd tau = s_tau;
-        for (int i = t; i < len; i += blockDim.x)
-            stab(AB, ldb, st + i, s, i == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0));
-        {
-            zd acc = dot8(D, b, v, o8, len, part, 0, o8 < len);
-            if (part == 0 && o8 < len) u[o8] = cmul(tau, acc);
-        }
-        __syncthreads();
-        sym_apply_store(D, b, len, v, u, tau, AB, ldb, st);
+        diag_update_store(D, dv, vr, vc, tau, len, partB, AB, ldb, st);
         publish(progress, s, 1);
         int k = 1;
         while (true) {
@@ -222,58 +190,54 @@ __global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n,
             if (J1 > n - 1) break;
             int J2 = min(ed + b, n - 1), lm = J2 - J1 + 1;
             if (s > 0 && !wait_progress(progress, s - 1, k + 2, err)) return;
-            // E = A[J1..J2, st..ed] and D = A[J1..J2, J1..J2] in one round trip
-            for (int idx = t; idx < lm * len; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                E[r + c * b] = ldab(AB, ldb, J1 + r, st + c);
+            // all loads of the task in flight at once
+            zd e0 = r < lm ? ldab(AB, ldb, J1 + r, st) : mk<double>(0, 0);  // E[:, 0], every warp
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) {
+                int c = w + HB_NW * i;
+                E[i] = r < lm && c < len ? ldab(AB, ldb, J1 + r, st + c) : mk<double>(0, 0);
             }
-            for (int idx = t; idx < lm * lm; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                D[r + c * b] = r >= c ? ldab(AB, ldb, J1 + r, J1 + c) : cconj(ldab(AB, ldb, J1 + c, J1 + r));
-            }
+            load_diag_block(D, AB, ldb, J1, lm);
+            // right application of the previous reflector: E <- E - (tau E v) v^H
+            zd ev = mk<double>(0, 0);
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) ev = cadd(ev, cmul(E[i], vc[i]));
+            partA[w][r] = ev;
             __syncthreads();
-            // right application of the previous reflector: E <- E - tau (E v) v^H
-            {
-                zd acc = dot8(E, b, v, o8, len, part, 0, o8 < lm);
-                if (part == 0 && o8 < lm) w[o8] = cmul(tau, acc);
+            zd wr = mk<double>(0, 0);
+#pragma unroll
+            for (int q = 0; q < HB_NW; q++) wr = cadd(wr, partA[q][r]);
+            wr = cmul(tau, wr);
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) E[i] = csub(E[i], cmul(wr, cconj(vc[i])));
+            e0 = csub(e0, wr);  // v[0] = 1
+            // new reflector from the updated first column (formed in every warp)
+            double beta2;
+            zd tau2;
+            zd v2r = larfg_lanes(e0, lm, &beta2, &tau2);
+            zd v2c[HB_NC];
+            zd dv2 = mk<double>(0, 0);
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) {
+                v2c[i] = shfl_z(v2r, w + HB_NW * i);
+                dv2 = cadd(dv2, cmul(D[i], v2c[i]));
             }
-            __syncthreads();
-            for (int idx = t; idx < lm * len; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                E[r + c * b] = csub(E[r + c * b], cmul(w[r], cconj(v[c])));
+            // left application to E: E <- E - v2 (conj(tau2) v2^H E), column 0 -> beta2 e_0
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) {
+                int c = w + HB_NW * i;
+                zd wl = warp_sum_z(cmulc(v2r, E[i]));
+                wl = cmul(cconj(tau2), wl);
+                if (r < lm && c < len) {
+                    zd val;
+                    if (c == 0) val = r == 0 ? mk<double>(beta2, 0.0) : mk<double>(0, 0);
+                    else val = csub(E[i], cmul(v2r, wl));
+                    stab(AB, ldb, J1 + r, st + c, val);
+                }
             }
-            __syncthreads();
-            // new reflector from E[:, 0]
-            if (t < 32) {
-                for (int i = t; i < lm; i += 32) v2[i] = E[i];
-                __syncwarp();
-                double beta;
-                zd t2;
-                larfg_warp(v2, lm, &beta, &t2);
-                if (t == 0) { s_beta = beta; s_tau = t2; }
-            }
-            __syncthreads();
-            zd tau2 = s_tau;
-            // left application coefficients and u = tau2 D v2 in the same phase
-            {
-                zd acc = dot8(E, b, v2, o8, lm, part, 1, o8 > 0 && o8 < len);
-                if (part == 0 && o8 > 0 && o8 < len) w[o8] = cmul(cconj(tau2), acc);
-                zd acc2 = dot8(D, b, v2, o8, lm, part, 0, o8 < lm);
-                if (part == 0 && o8 < lm) u[o8] = cmul(tau2, acc2);
-            }
-            __syncthreads();
-            for (int idx = t; idx < lm * len; idx += blockDim.x) {
-                int r = idx % lm, c = idx / lm;
-                zd val;
-                if (c == 0) val = r == 0 ? mk<double>(s_beta, 0.0) : mk<double>(0, 0);
-                else val = csub(E[r + c * b], cmul(v2[r], w[c]));
-                stab(AB, ldb, J1 + r, st + c, val);
-            }
-            __syncthreads();
-            sym_apply_store(D, b, lm, v2, u, tau2, AB, ldb, J1);
-            zd *tmp = v;
-            v = v2;
-            v2 = tmp;
+            diag_update_store(D, dv2, v2r, v2c, tau2, lm, partB, AB, ldb, J1);
+#pragma unroll
+            for (int i = 0; i < HB_NC; i++) vc[i] = v2c[i];
             tau = tau2;
             st = J1;
             ed = J2;
@@ -282,7 +246,6 @@ __global__ void __launch_bounds__(256) hb2st_kernel(double2 *AB, int ldb, int n,
             publish(progress, s, k);
         }
         publish(progress, s, PROGRESS_DONE);
-        __syncthreads();
     }
 }
 
@@ -600,9 +563,9 @@ extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *
     CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     CUDA_OK(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n, st));
     CUDA_OK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    if (b < 1 || b > 32) return qd_set_error(QD_ERR_UNSUPPORTED, "bulge chasing needs 1 <= b <= 32");
     void *args[] = {&AB, &ldb, &n, &b, &progress, &err};
-    size_t smem = (size_t)(2 * b * b + 4 * b) * sizeof(zd);
-    CUDA_OK(cudaFuncSetAttribute(hb2st_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 256, smem));
     if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
     int G = nsm * per_sm;
