@@ -94,13 +94,17 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
 }
 // Bounded wait on one phase.  Gives up after WAIT_NS or when another role
 // has raised the CTA's abort flag; returns false then.
+// The clock and the abort flag are read every 64 polls only: the waiting warps
+// of a CTA would otherwise keep the SM's conversion/special-register pipe busy.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
     if (mbar_try(bar, parity)) return true;
     unsigned long long t0 = now_ns();
-    for (;;) {
+    for (uint32_t it = 1;; it++) {
         if (mbar_try(bar, parity)) return true;
-        if (*abort_flag) return false;
-        if (now_ns() - t0 > WAIT_NS) return false;
+        if ((it & 63) == 0) {
+            if (*abort_flag) return false;
+            if (now_ns() - t0 > WAIT_NS) return false;
+        }
     }
 }
 
@@ -146,6 +150,15 @@ __device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint6
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
+// A operand from tensor memory (K-major: row i in lane i, element k in column k).
+__device__ __forceinline__ void umma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
@@ -164,6 +177,18 @@ __device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t *v) {
         : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Each lane of the warp writes 32 consecutive 32-bit columns of its own lane.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]),
+        "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]),
+        "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // Round to the nearest TF32 value (10 stored mantissa bits, ties away from
 // zero) with integer operations: add half an ulp of TF32 to the magnitude
@@ -256,30 +281,37 @@ __device__ __forceinline__ void ring_prev(int &s, uint32_t &ph, int n) {
 }
 __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
     unsigned long long t0 = now_ns();
-    while (!mbar_try(bar, parity) && now_ns() - t0 < WAIT_NS) {
-    }
+    for (uint32_t it = 1; !mbar_try(bar, parity); it++)
+        if ((it & 63) == 0 && now_ns() - t0 >= WAIT_NS) break;
 }
 
 // ---------------------------------------------------------------------------
 // X = A22 VT.  Three rings, each advanced once per k-block:
-//   A  (XA_STAGES x 16 KB): TMA fp32 tiles of A22, released as soon as the
-//      converter has read them, so that the ring turns over at DRAM latency;
-//   B  (XB_STAGES x 16 KB): TMA tiles of the right factor, hi and lo;
-//   L  (XL_STAGES x 32 KB): hi and lo of the A tile, written by the converter
-//      and read by the MMAs.
+//   A  (XA_STAGES x 16 KB smem): TMA fp32 tiles of A22, released as soon as
+//      the converter has read them, so that the ring turns over at DRAM latency;
+//   B  (XB_STAGES x 16 KB smem): TMA tiles of the right factor, hi and lo;
+//   L  (XL_STAGES x 64 TMEM columns): hi (columns 0-31) and lo (32-63) of the
+//      A tile, written by the converter with tcgen05.st (thread = row = TMEM
+//      lane) and read by the MMAs as their A operand, so the split tile never
+//      passes through shared memory: per k-block shared memory carries 16 KB
+//      in and out of the A ring and the B tiles, which keeps its bandwidth
+//      below the DRAM stream's.
 // The B tiles come from L2 and have their own producer so that their latency
 // is not serialised behind the converter.
 //   warp 0 A producer, warp 1 MMA, warps 2-5 epilogue, warps 6-9 converter,
 //   warp 10 B producer.
+// TMEM: columns [0, 128) two accumulators of 64, [128, 128 + 64 XL_STAGES) L.
 // ---------------------------------------------------------------------------
-constexpr int XA_STAGES = 6, XB_STAGES = 3, XL_STAGES = 2;
+constexpr int XA_STAGES = 8, XB_STAGES = 3, XL_STAGES = 4;
 constexpr int X_N = 64;
 constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
 constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB (hi or lo)
-constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES + XL_STAGES * 2 * X_A_BYTES;
+constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES;
 constexpr int X_CHUNK = 2;
 constexpr int X_WARPS = 11;
-constexpr int X_TMEM_COLS = 128;
+constexpr int X_L_COL0 = 2 * X_N;
+constexpr int X_TMEM_COLS = 512;
+static_assert(X_L_COL0 + 2 * BKF * XL_STAGES <= X_TMEM_COLS, "TMEM columns");
 
 __global__ void __launch_bounds__(X_WARPS * 32, 1)
     xprod_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -287,7 +319,6 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *ringA = smem, *ringB = smem + XA_STAGES * X_A_BYTES;
-    uint8_t *ringL = ringB + XB_STAGES * 2 * X_B_BYTES;
     uint64_t *fullA = (uint64_t *)(smem + X_SMEM);
     uint64_t *emptyA = fullA + XA_STAGES;
     uint64_t *fullB = emptyA + XA_STAGES;
@@ -403,16 +434,16 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     }
                     tc_fence_after();
                     const uint32_t d = tmem_base + (uint32_t)(ab * X_N);
-                    const uint32_t a_hi = smem_u32(ringL + sl * 2 * X_A_BYTES);
-                    const uint32_t a_lo = a_hi + X_A_BYTES;
+                    const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF);
+                    const uint32_t a_lo = a_hi + BKF;
                     const uint32_t b_hi = smem_u32(ringB + sb * 2 * X_B_BYTES), b_lo = b_hi + X_B_BYTES;
 #pragma unroll
                     for (int kk = 0; kk < BKF / 8; kk++) {
-                        uint32_t o = kk * 32;
+                        uint32_t o = kk * 32;  // bytes along K in the B tile
                         uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
-                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_hi + o), idesc, acc);
-                        umma_tf32(d, sw128_desc(a_hi + o), sw128_desc(b_lo + o), idesc, 1u);
-                        umma_tf32(d, sw128_desc(a_lo + o), sw128_desc(b_hi + o), idesc, 1u);
+                        umma_tf32_ts(d, a_hi + kk * 8, sw128_desc(b_hi + o), idesc, acc);
+                        umma_tf32_ts(d, a_hi + kk * 8, sw128_desc(b_lo + o), idesc, 1u);
+                        umma_tf32_ts(d, a_lo + kk * 8, sw128_desc(b_hi + o), idesc, 1u);
                     }
                     umma_commit(&emptyB[sb]);
                     umma_commit(&emptyL[sl]);
@@ -452,8 +483,10 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             }
         }
     } else {
-        // ---------------- converter: A fp32 -> hi and lo (L ring); releases the A slot ----------------
-        const int t = threadIdx.x - 6 * 32;  // 0..127
+        // ---------------- converter: A fp32 -> hi and lo in TMEM (L ring); releases the A slot ----------------
+        // Thread = row of the A tile = TMEM lane (warp w reaches lanes 32 (w % 4) ..).
+        const int q = warp & 3, row = q * 32 + lane;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)X_L_COL0;
         int sa = 0, sl = 0;
         uint32_t pa = 0, pl = 0;
         bool ok = true;
@@ -466,23 +499,29 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                     ok = false;
                     break;
                 }
-                const float4 *a = (const float4 *)(ringA + sa * X_A_BYTES);
-                float4 *ahi = (float4 *)(ringL + sl * 2 * X_A_BYTES);
-                float4 *alo = (float4 *)(ringL + sl * 2 * X_A_BYTES + X_A_BYTES);
+                tc_fence_after();
+                // row `row` of the 128-byte-swizzled tile: 16-byte chunk c sits at c ^ (row % 8)
+                const float4 *a = (const float4 *)(ringA + sa * X_A_BYTES) + row * 8;
+                float hi[BKF], lo[BKF];
 #pragma unroll
-                for (int u = 0; u < X_A_BYTES / 16 / 128; u++) {
-                    int idx = u * 128 + t;
-                    float4 x = a[idx], h, l;
-                    split3(x.x, h.x, l.x);
-                    split3(x.y, h.y, l.y);
-                    split3(x.z, h.z, l.z);
-                    split3(x.w, h.w, l.w);
-                    ahi[idx] = h;
-                    alo[idx] = l;
+                for (int c = 0; c < 8; c++) {
+                    float4 x = a[c ^ (row & 7)];
+                    split3(x.x, hi[4 * c], lo[4 * c]);
+                    split3(x.y, hi[4 * c + 1], lo[4 * c + 1]);
+                    split3(x.z, hi[4 * c + 2], lo[4 * c + 2]);
+                    split3(x.w, hi[4 * c + 3], lo[4 * c + 3]);
                 }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const uint32_t t = lane_base + (uint32_t)(sl * 2 * BKF);
+                tmem_st32(t, hi);
+                tmem_st32(t + BKF, lo);
+                tmem_st_wait();
+                tc_fence_before();
                 __syncwarp();
-                if ((threadIdx.x & 31) == 0) {  // one arrival per warp
+                // The A slot is released only now: the completed TMEM stores
+                // consumed every value read from it.  Released right after the
+                // loads, the next TMA tile (an async-proxy write) could land
+                // before loads delayed by other CTAs on the SM had read the slot.
+                if (lane == 0) {  // one arrival per warp
                     mbar_arrive(&emptyA[sa]);
                     mbar_arrive(&conv[sl]);
                 }
