@@ -16,14 +16,15 @@
 // Two products use it:
 //   qd_tc_xprod  X = A22 * VT (A22 Hermitian, full storage, complex64): A22's
 //                columns are read as K-major rows of conj(A22) = A22^T, so the
-//                big operand needs no transform; it is split hi/lo in shared
-//                memory by a converter warpgroup.  Split-K partials + reduce.
+//                big operand needs no transform; a converter warpgroup splits
+//                it hi/lo into tensor memory, where the MMAs read it.  Split-K
+//                partials + reduce.
 //   qd_tc_flush  A22 -= [V W] [W V]^H (the aggregated rank-2K update) on the
 //                lower-triangle tiles, mirrored into the upper triangle; both
 //                factors are small and are laid out and split once per call.
 //
 // Both kernels are persistent (one CTA per SM) and warp-specialised: TMA
-// producer(s), one MMA-issuing thread that also owns TMEM, epilogue warps
+// producer(s), MMA-issuing thread(s) (one owns TMEM), epilogue warps
 // that drain TMEM, and (xprod) a converter warpgroup.  The accumulator is
 // restarted every one or two k-blocks and summed in FP32 registers by the
 // epilogue, which keeps the tensor core's internal accumulation short.
@@ -298,9 +299,15 @@ __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
 //      below the DRAM stream's.
 // The B tiles come from L2 and have their own producer so that their latency
 // is not serialised behind the converter.
-//   warp 0 A producer, warp 1 MMA, warps 2-5 epilogue, warps 6-9 converter,
-//   warp 10 B producer.
-// TMEM: columns [0, 128) two accumulators of 64, [128, 128 + 64 XL_STAGES) L.
+// One thread issues at most about one MMA per 45 cycles, and a k-block takes
+// 12 MMAs (3 products x 4 steps of K = 8), so two threads issue them: warp 1
+// the steps 0-1, warp 11 the steps 2-3, each into its own accumulator; the
+// epilogue adds the two.  The barriers the MMAs release (emptyB, emptyL, tfull,
+// done) expect one commit from each issuer.
+//   warp 0 A producer, warps 1 and 11 MMA, warps 2-5 epilogue, warps 6-9
+//   converter, warp 10 B producer.
+// TMEM: columns [0, 256) the two issuers' double-buffered accumulators of 64
+// (issuer h, buffer ab at 128 h + 64 ab), [256, 256 + 64 XL_STAGES) L.
 // ---------------------------------------------------------------------------
 constexpr int XA_STAGES = 8, XB_STAGES = 3, XL_STAGES = 4;
 constexpr int X_N = 64;
@@ -308,10 +315,42 @@ constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
 constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB (hi or lo)
 constexpr int X_SMEM = XA_STAGES * X_A_BYTES + XB_STAGES * 2 * X_B_BYTES;
 constexpr int X_CHUNK = 2;
-constexpr int X_WARPS = 11;
-constexpr int X_L_COL0 = 2 * X_N;
+constexpr int X_WARPS = 12;
+constexpr int X_ISSUERS = 2;
+constexpr int X_L_COL0 = 2 * X_ISSUERS * X_N;
 constexpr int X_TMEM_COLS = 512;
 static_assert(X_L_COL0 + 2 * BKF * XL_STAGES <= X_TMEM_COLS, "TMEM columns");
+
+// Epilogue of the X product: every accumulation chunk is the sum of the two
+// issuers' accumulators (columns 64 (2 h + ab) of this warp's lane quarter).
+__device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t tmem_base, int q, int &ab,
+                                           uint32_t &aphase, uint64_t *tfull, uint64_t *tempty,
+                                           volatile int *abort_flag) {
+#pragma unroll
+    for (int c = 0; c < X_N; c++) acc[c] = 0.f;
+    for (int ch = 0; ch < nch; ch++) {
+        if (!mbar_wait_warp(&tfull[ab], aphase, abort_flag)) return false;
+        tc_fence_after();
+#pragma unroll
+        for (int h = 0; h < X_ISSUERS; h++) {
+            uint32_t v[X_N];
+            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((h * 2 + ab) * X_N);
+            tmem_ld32_issue(ta, v);
+            tmem_ld32_issue(ta + 32, v + 32);
+            tmem_ld_wait();
+#pragma unroll
+            for (int c = 0; c < X_N; c++) acc[c] += __uint_as_float(v[c]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(&tempty[ab]);  // one arrival per warp
+        if (++ab == 2) {
+            ab = 0;
+            aphase ^= 1;
+        }
+    }
+    return true;
+}
 
 __global__ void __launch_bounds__(X_WARPS * 32, 1)
     xprod_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -339,17 +378,17 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         }
         for (int s = 0; s < XB_STAGES; s++) {
             mbar_init(&fullB[s], 1);
-            mbar_init(&emptyB[s], 1);
+            mbar_init(&emptyB[s], X_ISSUERS);  // one commit per MMA issuer
         }
         for (int s = 0; s < XL_STAGES; s++) {
             mbar_init(&conv[s], 4);  // one arrival per converter warp
-            mbar_init(&emptyL[s], 1);
+            mbar_init(&emptyL[s], X_ISSUERS);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&tfull[b], 1);
+            mbar_init(&tfull[b], X_ISSUERS);
             mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
-        mbar_init(done, 1);
+        mbar_init(done, X_ISSUERS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -407,10 +446,12 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                 wait_bounded(&full[s], ph);
             }
         }
-    } else if (warp == 1) {
-        // ---------------- MMA issuer (accumulation restarted every X_CHUNK k-blocks) ----------------
+    } else if (warp == 1 || warp == 11) {
+        // ---------------- MMA issuers (accumulation restarted every X_CHUNK k-blocks) ----------------
         if (lane == 0) {
+            const int h = warp == 11;  // K steps 2h, 2h + 1 of every k-block
             const uint32_t idesc = tf32_idesc(TILE_M, X_N);
+            const uint64_t bdesc0 = sw128_desc(smem_u32(ringB));
             int sb = 0, sl = 0, ab = 0;
             uint32_t pb = 0, pl = 0, aphase = 0;
             bool ok = true;
@@ -433,17 +474,18 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d = tmem_base + (uint32_t)(ab * X_N);
-                    const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF);
+                    const uint32_t d = tmem_base + (uint32_t)((h * 2 + ab) * X_N);
+                    const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF + h * 16);
                     const uint32_t a_lo = a_hi + BKF;
-                    const uint32_t b_hi = smem_u32(ringB + sb * 2 * X_B_BYTES), b_lo = b_hi + X_B_BYTES;
+                    // +32 bytes along K in the B tile = +2 in the descriptor's address field
+                    const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES + h * 64) >> 4);
+                    const uint64_t bl = bh + (X_B_BYTES >> 4);
 #pragma unroll
-                    for (int kk = 0; kk < BKF / 8; kk++) {
-                        uint32_t o = kk * 32;  // bytes along K in the B tile
+                    for (int kk = 0; kk < 2; kk++) {
                         uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
-                        umma_tf32_ts(d, a_hi + kk * 8, sw128_desc(b_hi + o), idesc, acc);
-                        umma_tf32_ts(d, a_hi + kk * 8, sw128_desc(b_lo + o), idesc, 1u);
-                        umma_tf32_ts(d, a_lo + kk * 8, sw128_desc(b_hi + o), idesc, 1u);
+                        umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc, acc);
+                        umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
+                        umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
                     }
                     umma_commit(&emptyB[sb]);
                     umma_commit(&emptyL[sl]);
@@ -470,8 +512,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             int tm, sp, kb0, kb1;
             xprod_item(args, item, tm, sp, kb0, kb1);
             float acc[X_N];
-            if (!drain_item<X_N, X_N>(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, 0, ab, aphase, tfull,
-                                      tempty, abort_flag)) {
+            if (!drain_pair(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, ab, aphase, tfull, tempty,
+                            abort_flag)) {
                 fail(4);
                 break;
             }
