@@ -739,20 +739,33 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
             float2 *Crow = args.C + row;                            // C[row, :]
             float2 *Ccol = args.C + (int64_t)row * args.ldc;        // C[:, row] (mirror)
             const int col0 = tn * (F_N / 2) + cbase / 2;
+            // Batches of F_LD columns: all loads of a batch are issued before its
+            // stores (a store may alias a later load, so the compiler would
+            // otherwise keep every load behind the previous store).
+            constexpr int F_LD = 8;
 #pragma unroll
-            for (int jj = 0; jj < F_EPI_COLS / 2; jj++) {
-                const int col = col0 + jj;
-                if (col >= args.cols || col > row) continue;
-                float2 *p = Crow + (int64_t)col * args.ldc;
-                float2 c = *p;
-                c.x -= acc[2 * jj];
-                c.y -= acc[2 * jj + 1];
-                if (col == row) {
-                    c.y = 0.f;
-                    *p = c;
-                } else {
-                    *p = c;
-                    Ccol[col] = make_float2(c.x, -c.y);
+            for (int j0 = 0; j0 < F_EPI_COLS / 2; j0 += F_LD) {
+                float2 cv[F_LD];
+#pragma unroll
+                for (int j = 0; j < F_LD; j++) {
+                    const int col = col0 + j0 + j;
+                    cv[j] = (col < args.cols && col <= row) ? __ldcg(Crow + (int64_t)col * args.ldc)
+                                                            : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int j = 0; j < F_LD; j++) {
+                    const int col = col0 + j0 + j;
+                    if (col >= args.cols || col > row) continue;
+                    float2 c = cv[j];
+                    c.x -= acc[2 * (j0 + j)];
+                    c.y -= acc[2 * (j0 + j) + 1];
+                    if (col == row) {
+                        c.y = 0.f;
+                        Crow[(int64_t)col * args.ldc] = c;
+                    } else {
+                        Crow[(int64_t)col * args.ldc] = c;
+                        Ccol[col] = make_float2(c.x, -c.y);
+                    }
                 }
             }
         }
