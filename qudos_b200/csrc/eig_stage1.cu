@@ -69,6 +69,41 @@ __device__ void panel_partials(const cpx<R> *tile, int chunk, int r0, int rows, 
     }
 }
 
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide arrival on a counter that only grows (zeroed by the host before the
+// launch): barrier number j completes when the counter reaches (j + 1) * G.  The
+// block barrier plus the release add publish every thread's prior stores; the
+// acquire poll is bounded.
+__device__ __forceinline__ bool grid_arrive_wait(unsigned *ctr, unsigned target, int *err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
+        long long it = 0;
+        while (ld_acquire_u32(ctr) < target) {
+            if (++it > QD_BAR_LIMIT || *(volatile int *)err) {
+                atomicExch(err, 6);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Panel QR.  Per reflector j: one grid arrival, then every block reduces the
+// column's partial sums, forms the Householder scalars and updates its rows.
+// The update does column j+1 first; the remaining columns are updated in one
+// pass that also accumulates column j+1's partial sums for the next reflector
+// (warps over columns, lanes over rows: no index division).
 template <typename R>
 __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, int m, int nb, int nref, int chunk,
                                                        cpx<R> *Rout, cpx<R> *tau_out, double2 *red,
@@ -84,32 +119,28 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
     const int r0 = blockIdx.x * chunk;
     const int rows = max(0, min(m, r0 + chunk) - r0);
     const int stride = nb + 1;  // double2 slots per block per buffer
-    for (int idx = threadIdx.x; idx < rows * nb; idx += blockDim.x) {
-        int c = idx / rows, rr = idx % rows;
-        tile[c * chunk + rr] = A[(int64_t)(r0 + rr) + (int64_t)c * lda];
-    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int c = w; c < nb; c += nw)
+        for (int rr = lane; rr < rows; rr += 32) tile[c * chunk + rr] = A[(int64_t)(r0 + rr) + (int64_t)c * lda];
     __syncthreads();
     panel_partials<R>(tile, chunk, r0, rows, nb, 0, red + (size_t)blockIdx.x * stride, rowbuf);
     for (int j = 0; j < nref; j++) {
         const int buf = j & 1;
         double2 *redb = red + (size_t)buf * G * stride;
         double2 *rowb = rowbuf + (size_t)buf * nb;
-        if (!grid_barrier(bar, G, err, QD_BAR_LIMIT)) return;
+        if (!grid_arrive_wait(bar, (unsigned)(j + 1) * G, err)) return;
         // ---- reduce the partials of column j over all blocks (one warp per value)
-        {
-            int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-            for (int slot = w; slot < nb - j; slot += nw) {
-                int s = slot == 0 ? 0 : j + slot;
-                double sr = 0.0, si = 0.0;
-                for (unsigned q = lane; q < G; q += 32) {
-                    double2 v = __ldcg(&redb[(size_t)q * stride + s]);
-                    sr += v.x;
-                    si += v.y;
-                }
-                sr = warp_sum(sr);
-                si = warp_sum(si);
-                if (lane == 0) s_red[slot] = make_double2(sr, si);
+        for (int slot = w; slot < nb - j; slot += nw) {
+            int sidx = slot == 0 ? 0 : j + slot;
+            double sr = 0.0, si = 0.0;
+            for (unsigned q = lane; q < G; q += 32) {
+                double2 v = __ldcg(&redb[(size_t)q * stride + sidx]);
+                sr += v.x;
+                si += v.y;
             }
+            sr = warp_sum(sr);
+            si = warp_sum(si);
+            if (lane == 0) s_red[slot] = make_double2(sr, si);
         }
         __syncthreads();
         // ---- Householder scalars (LAPACK zlarfg conventions)
@@ -140,18 +171,50 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
             s_w[c] = make_double2(tr * wr - ti * wi, tr * wi + ti * wr);
         }
         __syncthreads();
-        // ---- A[r, c] -= v_r s_w[c] for r >= j, c > j  (v_j = 1, v_r = scale x_r)
+        // ---- A[r, c] -= v_r s_w[c] for r >= j, c > j  (v_j = 1, v_r = scale x_r for r > j)
         const cpx<R> scale = mk<R>((R)s_scale.x, (R)s_scale.y);
-        for (int idx = threadIdx.x; idx < rows * (nb - j - 1); idx += blockDim.x) {
-            int c = j + 1 + idx / rows, rr = idx % rows;
-            int r = r0 + rr;
-            if (r < j) continue;
-            cpx<R> v = (r == j) ? mk<R>(1, 0) : cmul(tile[j * chunk + rr], scale);
-            cpx<R> tw = mk<R>((R)s_w[c].x, (R)s_w[c].y);
-            tile[c * chunk + rr] = csub(tile[c * chunk + rr], cmul(v, tw));
+        const bool nextp = j + 1 < nref;
+        if (j + 1 < nb) {
+            const cpx<R> tw = mk<R>((R)s_w[j + 1].x, (R)s_w[j + 1].y);
+            for (int rr = threadIdx.x; rr < rows; rr += blockDim.x) {
+                const int r = r0 + rr;
+                if (r < j) continue;
+                cpx<R> v = (r == j) ? mk<R>(1, 0) : cmul(tile[j * chunk + rr], scale);
+                tile[(j + 1) * chunk + rr] = csub(tile[(j + 1) * chunk + rr], cmul(v, tw));
+            }
         }
         __syncthreads();
-        // ---- column j becomes v (explicit); row j of R is final
+        double2 *redn = red + (size_t)((j + 1) & 1) * G * stride + (size_t)blockIdx.x * stride;
+        for (int c = j + 1 + w; c < nb; c += nw) {
+            const bool upd = c > j + 1;
+            const cpx<R> tw = upd ? mk<R>((R)s_w[c].x, (R)s_w[c].y) : mk<R>(0, 0);
+            double sr = 0.0, si = 0.0;
+            for (int rr = lane; rr < rows; rr += 32) {
+                const int r = r0 + rr;
+                cpx<R> a = tile[c * chunk + rr];
+                if (upd && r >= j) {
+                    cpx<R> v = (r == j) ? mk<R>(1, 0) : cmul(tile[j * chunk + rr], scale);
+                    a = csub(a, cmul(v, tw));
+                    tile[c * chunk + rr] = a;
+                }
+                if (nextp && r > j + 1) {
+                    cpx<R> x = tile[(j + 1) * chunk + rr];
+                    if (!upd) {
+                        sr += (double)x.re * x.re + (double)x.im * x.im;
+                    } else {
+                        sr += (double)x.re * a.re + (double)x.im * a.im;
+                        si += (double)x.re * a.im - (double)x.im * a.re;
+                    }
+                }
+            }
+            if (nextp) {
+                sr = warp_sum(sr);
+                si = warp_sum(si);
+                if (lane == 0) __stcg(&redn[upd ? c : 0], make_double2(sr, si));
+            }
+        }
+        __syncthreads();
+        // ---- column j becomes v (explicit); row j of R is final; row j+1 is published
         for (int rr = threadIdx.x; rr < rows; rr += blockDim.x)
             if (r0 + rr > j) tile[j * chunk + rr] = cmul(tile[j * chunk + rr], scale);
         if (j >= r0 && j < r0 + rows) {
@@ -163,21 +226,23 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
             }
             if (threadIdx.x == 0) tau_out[j] = mk<R>((R)s_tau.x, (R)s_tau.y);
         }
-        __syncthreads();
-        if (j + 1 < nref)
-            panel_partials<R>(tile, chunk, r0, rows, nb, j + 1,
-                              red + (size_t)((j + 1) & 1) * G * stride + (size_t)blockIdx.x * stride,
-                              rowbuf + (size_t)((j + 1) & 1) * nb);
+        if (nextp && j + 1 >= r0 && j + 1 < r0 + rows) {
+            int rr = j + 1 - r0;
+            double2 *rown = rowbuf + (size_t)((j + 1) & 1) * nb;
+            for (int c = j + 1 + threadIdx.x; c < nb; c += blockDim.x) {
+                cpx<R> a = tile[c * chunk + rr];
+                __stcg(&rown[c], make_double2((double)a.re, (double)a.im));
+            }
+        }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < rows * nb; idx += blockDim.x) {
-        int c = idx / rows, rr = idx % rows;
-        int r = r0 + rr;
-        if (c >= nref) continue;  // only the reflector columns are kept (R is in Rout)
-        cpx<R> v = tile[c * chunk + rr];
-        if (r < c) v = mk<R>(0, 0);
-        A[(int64_t)r + (int64_t)c * lda] = v;
-    }
+    for (int c = w; c < nref; c += nw)
+        for (int rr = lane; rr < rows; rr += 32) {
+            const int r = r0 + rr;
+            cpx<R> v = tile[c * chunk + rr];
+            if (r < c) v = mk<R>(0, 0);
+            A[(int64_t)r + (int64_t)c * lda] = v;
+        }
 }
 
 // T of the compact WY form (LAPACK zlarft, forward, columnwise):
