@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
     cpx<R> *tile = (cpx<R> *)smem_raw;  // [nb][chunk]
     __shared__ double2 s_red[64];
     __shared__ double2 s_w[64];
+    __shared__ double2 s_row[64];  // row j of the panel, columns j ..
     __shared__ double s_beta;
     __shared__ double2 s_tau, s_scale;
     const unsigned G = gridDim.x;
@@ -129,7 +130,9 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
         double2 *redb = red + (size_t)buf * G * stride;
         double2 *rowb = rowbuf + (size_t)buf * nb;
         if (!grid_arrive_wait(bar, (unsigned)(j + 1) * G, err)) return;
-        // ---- reduce the partials of column j over all blocks (one warp per value)
+        // ---- reduce the partials of column j over all blocks (one warp per value);
+        //      row j is fetched in the same round trip
+        const double2 rv = (int)threadIdx.x < nb - j ? __ldcg(&rowb[j + threadIdx.x]) : make_double2(0.0, 0.0);
         for (int slot = w; slot < nb - j; slot += nw) {
             int sidx = slot == 0 ? 0 : j + slot;
             double sr = 0.0, si = 0.0;
@@ -142,11 +145,12 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
             si = warp_sum(si);
             if (lane == 0) s_red[slot] = make_double2(sr, si);
         }
+        if ((int)threadIdx.x < nb - j) s_row[threadIdx.x] = rv;
         __syncthreads();
         // ---- Householder scalars (LAPACK zlarfg conventions)
         if (threadIdx.x == 0) {
             double sig = s_red[0].x;
-            double2 a = __ldcg(&rowb[j]);
+            double2 a = s_row[0];
             double ar = a.x, ai = a.y;
             if (sig == 0.0 && ai == 0.0) {
                 s_tau = make_double2(0.0, 0.0);
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
         __syncthreads();
         // ---- w_c = A[j,c] + conj(scale) (x^H A_c);  s_w = conj(tau) w_c
         for (int c = j + 1 + threadIdx.x; c < nb; c += blockDim.x) {
-            double2 a = __ldcg(&rowb[c]);
+            double2 a = s_row[c - j];
             double2 d = s_red[c - j];
             double sr = s_scale.x, si = -s_scale.y;  // conj(scale)
             double wr = a.x + sr * d.x - si * d.y, wi = a.y + sr * d.y + si * d.x;
@@ -246,34 +250,37 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
 }
 
 // T of the compact WY form (LAPACK zlarft, forward, columnwise):
-// T[i,i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i].  One block.
+// T[i,i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i].  One block;
+// the Gram matrix is staged in shared memory first (dynamic: 2 nb^2 double2),
+// so the sequential recursion over i never waits on global memory.
 template <typename R>
 __global__ void form_t_kernel(const cpx<R> *gram, int ldg, const cpx<R> *tau, cpx<R> *T, int ldt, int nb) {
-    __shared__ double Tl[2 * 48 * 48];  // nb <= 48
+    extern __shared__ double2 ft_smem[];
+    double2 *Tl = ft_smem;            // nb x nb
+    double2 *Gs = ft_smem + nb * nb;  // nb x nb
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
         int p = idx % nb, q = idx / nb;
-        Tl[2 * idx] = p == q ? (double)tau[p].re : 0.0;
-        Tl[2 * idx + 1] = p == q ? (double)tau[p].im : 0.0;
+        Tl[idx] = p == q ? make_double2((double)tau[p].re, (double)tau[p].im) : make_double2(0.0, 0.0);
+        cpx<R> g = gram[p + (int64_t)q * ldg];
+        Gs[idx] = make_double2((double)g.re, (double)g.im);
     }
     __syncthreads();
     for (int i = 1; i < nb; i++) {
-        double tr = Tl[2 * (i + i * nb)], ti = Tl[2 * (i + i * nb) + 1];
+        const double2 t = Tl[i + i * nb];
         for (int p = threadIdx.x; p < i; p += blockDim.x) {
             double sr = 0.0, si = 0.0;
             for (int q = p; q < i; q++) {
-                double a_r = Tl[2 * (p + q * nb)], a_i = Tl[2 * (p + q * nb) + 1];
-                cpx<R> g = gram[q + (int64_t)i * ldg];
-                sr += a_r * g.re - a_i * g.im;
-                si += a_r * g.im + a_i * g.re;
+                const double2 a = Tl[p + q * nb], g = Gs[q + i * nb];
+                sr += a.x * g.x - a.y * g.y;
+                si += a.x * g.y + a.y * g.x;
             }
-            Tl[2 * (p + i * nb)] = -(tr * sr - ti * si);
-            Tl[2 * (p + i * nb) + 1] = -(tr * si + ti * sr);
+            Tl[p + i * nb] = make_double2(-(t.x * sr - t.y * si), -(t.x * si + t.y * sr));
         }
         __syncthreads();
     }
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
         int p = idx % nb, q = idx / nb;
-        T[p + (int64_t)q * ldt] = mk<R>((R)Tl[2 * idx], (R)Tl[2 * idx + 1]);
+        T[p + (int64_t)q * ldt] = mk<R>((R)Tl[idx].x, (R)Tl[idx].y);
     }
 }
 
@@ -473,7 +480,17 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         prof_mark(2, st);
         BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, m, &one, P, lda, P, lda, &zero, (T *)w.gram, b));
         qd_count_launch(1);
-        form_t_kernel<R><<<1, 256, 0, st>>>((const cpx<R> *)w.gram, b, (const cpx<R> *)w.tau, (cpx<R> *)Tp, b, nb);
+        {
+            static int ft_configured[2] = {0, 0};
+            const int ti = sizeof(R) == 8 ? 0 : 1;
+            if (!ft_configured[ti]) {  // nb <= 48: up to 72 KB
+                CUDA_OK(cudaFuncSetAttribute(form_t_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             2 * 48 * 48 * (int)sizeof(double2)));
+                ft_configured[ti] = 1;
+            }
+        }
+        form_t_kernel<R><<<1, 256, 2 * nb * nb * sizeof(double2), st>>>((const cpx<R> *)w.gram, b,
+                                                                        (const cpx<R> *)w.tau, (cpx<R> *)Tp, b, nb);
         CUDA_OK(cudaGetLastError());
         // 4. VT = V T ; 5. X = A22 VT (stale A22 + pending terms), written straight into Wacc
         T *VT = (T *)w.VT;
