@@ -302,14 +302,17 @@ __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
 // One thread issues at most about one MMA per 45 cycles, and a k-block takes
 // 12 MMAs (3 products x 4 steps of K = 8), so two threads issue them: warp 1
 // the steps 0-1, warp 11 the steps 2-3, each into its own accumulator; the
-// epilogue adds the two.  The barriers the MMAs release (emptyB, emptyL, tfull,
-// done) expect one commit from each issuer.
+// epilogue adds the two.  The B ring and the L ring have the same depth and
+// advance together, so one barrier per stage (emptyL) frees both the B tile and
+// the TMEM stage: each issuer commits once per k-block.  The barriers the MMAs
+// release (emptyL, tfull, done) expect one commit from each issuer.
 //   warp 0 A producer, warps 1 and 11 MMA, warps 2-5 epilogue, warps 6-9
 //   converter, warp 10 B producer.
 // TMEM: columns [0, 256) the two issuers' double-buffered accumulators of 64
 // (issuer h, buffer ab at 128 h + 64 ab), [256, 256 + 64 XL_STAGES) L.
 // ---------------------------------------------------------------------------
-constexpr int XA_STAGES = 8, XB_STAGES = 3, XL_STAGES = 4;
+constexpr int XA_STAGES = 8, XB_STAGES = 4, XL_STAGES = 4;
+static_assert(XB_STAGES == XL_STAGES, "the B and L rings share their release barrier");
 constexpr int X_N = 64;
 constexpr int X_A_BYTES = TILE_M * BKF * 4;  // 16 KB
 constexpr int X_B_BYTES = X_N * BKF * 4;     // 8 KB (hi or lo)
@@ -361,8 +364,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
     uint64_t *fullA = (uint64_t *)(smem + X_SMEM);
     uint64_t *emptyA = fullA + XA_STAGES;
     uint64_t *fullB = emptyA + XA_STAGES;
-    uint64_t *emptyB = fullB + XB_STAGES;
-    uint64_t *conv = emptyB + XB_STAGES;
+    uint64_t *conv = fullB + XB_STAGES;
     uint64_t *emptyL = conv + XL_STAGES;
     uint64_t *tfull = emptyL + XL_STAGES;
     uint64_t *tempty = tfull + 2;
@@ -376,10 +378,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             mbar_init(&fullA[s], 1);
             mbar_init(&emptyA[s], 4);  // released by the four converter warps
         }
-        for (int s = 0; s < XB_STAGES; s++) {
-            mbar_init(&fullB[s], 1);
-            mbar_init(&emptyB[s], X_ISSUERS);  // one commit per MMA issuer
-        }
+        for (int s = 0; s < XB_STAGES; s++) mbar_init(&fullB[s], 1);
         for (int s = 0; s < XL_STAGES; s++) {
             mbar_init(&conv[s], 4);  // one arrival per converter warp
             mbar_init(&emptyL[s], X_ISSUERS);
@@ -412,7 +411,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         if (lane == 0) {
             const bool isA = warp == 0;
             const int nst = isA ? XA_STAGES : XB_STAGES;
-            uint64_t *full = isA ? fullA : fullB, *empty = isA ? emptyA : emptyB;
+            uint64_t *full = isA ? fullA : fullB, *empty = isA ? emptyA : emptyL;
             int s = 0;
             uint32_t ph = 0;
             long issued = 0;
@@ -487,8 +486,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
                         umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
                     }
-                    umma_commit(&emptyB[sb]);
-                    umma_commit(&emptyL[sl]);
+                    umma_commit(&emptyL[sl]);  // frees B stage sb == sl and TMEM stage sl
                     ring_next(sb, pb, XB_STAGES);
                     ring_next(sl, pl, XL_STAGES);
                     if (cpos == X_CHUNK - 1 || kb == kb1 - 1) {
