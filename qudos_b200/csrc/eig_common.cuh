@@ -1,5 +1,5 @@
 // Shared pieces of the eigensolver kernels: complex scalar templates, block
-// reductions and a bounded grid barrier for cooperative launches.
+// reductions and the stage-1 workspace.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -65,39 +65,4 @@ __device__ __forceinline__ double block_sum(double v, double *scratch) {
     }
     __syncthreads();
     return scratch[32];
-}
-
-// Grid barrier for kernels launched cooperatively (all blocks co-resident).
-// bar[0] counts arrivals, bar[1] is the generation.  The wait is bounded: after
-// `limit` polls the block records QD_ERR_TIMEOUT-style failure in *err and the
-// barrier returns false, so a kernel whose peer has died exits instead of
-// hanging.
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err, long long limit) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile unsigned *gen = bar + 1;
-        unsigned g = *gen;
-        __threadfence();
-        unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            long long it = 0;
-            while (*gen == g) {
-                if (++it > limit || *(volatile int *)err) {
-                    atomicExch(err, 6);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
 }
