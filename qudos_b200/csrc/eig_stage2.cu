@@ -348,14 +348,21 @@ __device__ __forceinline__ zd band_val(const double2 *AB, int ldb, int b, int n,
     return v;
 }
 
+#define IW_ROWS 64
+#define IW_COLS 128
+#define IW(i, c) ((((i) & (IW_ROWS - 1)) * IW_COLS) + ((c) & (IW_COLS - 1)))
+
 __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int ldb, int n, int b, const double *lam,
                                                          const int *group_start, const int *group_size, double2 *Lw,
                                                          double2 *Uw, int *ipivw, double2 *Z, int64_t ldz,
                                                          double bnorm, double2 *ywork) {
     extern __shared__ unsigned char sm_raw[];
-    const int rows = b + 1, cols = 2 * b + 1;
-    zd *W = (zd *)sm_raw;                 // [rows][cols] circular window
-    zd *lcol = W + rows * cols;           // b multipliers of the current step
+    const int cols = 2 * b + 1;
+    // Circular window of the banded LU, 64 row slots x 128 column slots (b <= 32):
+    // (i, c) lives in W[IW(i, c)].  The live rows j..j+b and columns j..j+2b
+    // never share a slot with the row and column that enter at step j.
+    zd *W = (zd *)sm_raw;
+    zd *lcol = W + IW_ROWS * IW_COLS;  // b multipliers of the current step
     __shared__ double scratch[33];
     __shared__ int s_piv;
     __shared__ zd s_inv;
@@ -365,21 +372,32 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
     double2 *L = Lw + (int64_t)g * n * b;
     double2 *U = Uw + (int64_t)g * n * cols;
     int *ipiv = ipivw + (int64_t)g * n;
-    // window slot of (i, c): W[(i % rows) * cols + (c % cols)]
-    for (int idx = threadIdx.x; idx < rows * cols; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < (b + 1) * cols; idx += blockDim.x) {
         int i = idx / cols, c = idx % cols;
-        W[(i % rows) * cols + (c % cols)] = band_val(AB, ldb, b, n, i, c, lambda);
+        W[IW(i, c)] = band_val(AB, ldb, b, n, i, c, lambda);
     }
+    // Values entering at step j (original matrix entries, so fetched one step
+    // ahead): thread t < 2b+1 holds (j+b+1, j+1+t), thread 2b+1+k (k < b)
+    // holds (j+1+k, j+2b+1).
+    auto incoming = [&](int j) -> zd {
+        const int t = threadIdx.x;
+        if (t < cols) return band_val(AB, ldb, b, n, j + b + 1, j + 1 + t, lambda);
+        if (t < cols + b) return band_val(AB, ldb, b, n, j + 1 + (t - cols), j + 2 * b + 1, lambda);
+        return mk<double>(0, 0);
+    };
+    zd in_next = incoming(0);
     __syncthreads();
     const double tiny = 2.220446049250313e-16 * bnorm;
     for (int j = 0; j < n; j++) {
         int imax = min(j + b, n - 1), cmax = min(j + 2 * b, n - 1);
+        const zd in_cur = in_next;
+        if (j + 1 < n) in_next = incoming(j + 1);
         if (threadIdx.x < 32) {
             // pivot search in column j, rows j..imax
             double best = -1.0;
             int bi = j;
             for (int i = j + threadIdx.x; i <= imax; i += 32) {
-                double a = cabs2(W[(i % rows) * cols + (j % cols)]);
+                double a = cabs2(W[IW(i, j)]);
                 if (a > best) { best = a; bi = i; }
             }
             for (int o = 16; o > 0; o >>= 1) {
@@ -392,50 +410,51 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
             int p = bi;
             if (p != j) {
                 for (int c = j + threadIdx.x; c <= cmax; c += 32) {
-                    zd t = W[(j % rows) * cols + (c % cols)];
-                    W[(j % rows) * cols + (c % cols)] = W[(p % rows) * cols + (c % cols)];
-                    W[(p % rows) * cols + (c % cols)] = t;
+                    zd t = W[IW(j, c)];
+                    W[IW(j, c)] = W[IW(p, c)];
+                    W[IW(p, c)] = t;
                 }
             }
             __syncwarp();
             if (threadIdx.x == 0) {
-                zd piv = W[(j % rows) * cols + (j % cols)];
+                zd piv = W[IW(j, j)];
                 double a2 = cabs2(piv);
                 if (a2 < tiny * tiny) {
                     piv = mk<double>(tiny, 0.0);
-                    W[(j % rows) * cols + (j % cols)] = piv;
+                    W[IW(j, j)] = piv;
                     a2 = tiny * tiny;
                 }
                 s_inv = mk<double>(piv.re / a2, -piv.im / a2);
             }
             __syncwarp();
             for (int i = j + 1 + threadIdx.x; i <= imax; i += 32) {
-                zd l = cmul(W[(i % rows) * cols + (j % cols)], s_inv);
+                zd l = cmul(W[IW(i, j)], s_inv);
                 lcol[i - j - 1] = l;
                 L[(int64_t)j * b + (i - j - 1)] = make_double2(l.re, l.im);
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) ipiv[j] = s_piv;
-        // U row j and the rank-1 update of the trailing window
+        // U row j, the rank-1 update of the live window (lanes along columns,
+        // four row groups) and the entering row and column, all in one phase
         for (int c = j + threadIdx.x; c < j + cols; c += blockDim.x) {
-            zd u = c <= cmax ? W[(j % rows) * cols + (c % cols)] : mk<double>(0, 0);
+            zd u = c <= cmax ? W[IW(j, c)] : mk<double>(0, 0);
             U[(int64_t)j * cols + (c - j)] = make_double2(u.re, u.im);
         }
-        int nr = imax - j, nc = cmax - j;
-        for (int idx = threadIdx.x; idx < nr * nc; idx += blockDim.x) {
-            int i = j + 1 + idx % nr, c = j + 1 + idx / nr;
-            zd *a = &W[(i % rows) * cols + (c % cols)];
-            *a = csub(*a, cmul(lcol[i - j - 1], W[(j % rows) * cols + (c % cols)]));
+        const int nr = imax - j, nc = cmax - j;
+        {
+            const int cc = threadIdx.x & 63, rg = threadIdx.x >> 6;
+            if (cc < nc) {
+                const int c = j + 1 + cc;
+                const zd top = W[IW(j, c)];
+                for (int ri = rg; ri < nr; ri += 4) {
+                    zd *a = &W[IW(j + 1 + ri, c)];
+                    *a = csub(*a, cmul(lcol[ri], top));
+                }
+            }
         }
-        __syncthreads();
-        // slide the window: row j leaves (slot reused by row j+b+1), column j leaves (slot for j+2b+1)
-        int nrow = j + b + 1, ncol = j + 2 * b + 1;
-        for (int c = j + 1 + threadIdx.x; c <= j + 2 * b + 1; c += blockDim.x)
-            W[(nrow % rows) * cols + (c % cols)] = band_val(AB, ldb, b, n, nrow, c, lambda);
-        __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < j + b + 1; i += blockDim.x)
-            W[(i % rows) * cols + (ncol % cols)] = band_val(AB, ldb, b, n, i, ncol, lambda);
+        if ((int)threadIdx.x < cols) W[IW(j + b + 1, j + 1 + threadIdx.x)] = in_cur;
+        else if ((int)threadIdx.x < cols + b) W[IW(j + 1 + (threadIdx.x - cols), j + 2 * b + 1)] = in_cur;
         __syncthreads();
     }
     // ---- inverse iteration on the group's block of vectors (one warp per vector).
@@ -594,7 +613,8 @@ extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const do
                              const int *gstart_dev, const int *gsize_dev, double2 *Lw, double2 *Uw, int *ipivw,
                              double2 *Z, int64_t ldz, double bnorm, double2 *ywork, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    size_t smem = (size_t)((b + 1) * (2 * b + 1) + b + 8 * 192) * sizeof(zd);
+    if (b < 1 || b > 32) return qd_set_error(QD_ERR_UNSUPPORTED, "band inverse iteration needs 1 <= b <= 32");
+    size_t smem = (size_t)(IW_ROWS * IW_COLS + b + 8 * 192) * sizeof(zd);
     CUDA_OK(cudaFuncSetAttribute(band_invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     qd_count_launch(1);
     band_invit_kernel<<<ngroups, 256, smem, st>>>(AB0, ldb, n, b, lam_dev, gstart_dev, gsize_dev, Lw, Uw, ipivw, Z,
