@@ -144,8 +144,8 @@ def run_reference(args, ws, rank):
 
 
 # DRAM bytes per launch of xprod_kernel over its algorithmic bytes, from the ncu
-# capture summarised in profiles/xprod_kernel_mg4.txt (one launch, m = 5480).
-XPROD_TRAFFIC_RATIO = 1.086
+# capture summarised in profiles/xprod_kernel_9cubed.md (one launch, m = 5480).
+XPROD_TRAFFIC_RATIO = 1.083
 
 
 def tc_stats(L, which):
