@@ -7,10 +7,12 @@
 // k..k+b-1, rows k+b..N-1):
 //   * panel_qr_kernel: Householder QR of the tall panel in one cooperative
 //     launch.  Each block keeps its slice of rows in shared memory for all b
-//     columns.  Per column there is exactly one bounded grid barrier: the
-//     column norm and the dot products with the remaining columns are formed
-//     from the unscaled column in the same pass (w_c = A[j,c] + conj(s) x^H A_c),
-//     double-buffered in global scratch and reduced by whole warps.
+//     columns.  Per column there is exactly one bounded grid arrival (a
+//     counter that only grows): the column norm and the dot products with the
+//     remaining columns are formed from the unscaled column
+//     (w_c = A[j,c] + conj(s) x^H A_c), accumulated in the pass that applies
+//     the previous reflector, double-buffered in global scratch and reduced by
+//     whole warps.
 //   * T of the compact WY form I - V T V^H from the Gram matrix V^H V (GEMM)
 //     and the tau's (form_t_kernel).
 //   * delayed trailing update: the two-sided update A22 <- Q^H A22 Q is written
@@ -19,7 +21,8 @@
 //     trailing matrix in one rank-2*agg update; in between, the next panel's
 //     columns and X are corrected for the pending terms with thin GEMMs.
 //     FP64: ZHEMM/ZHER2K on the lower triangle.  complex64 (mixed path): the
-//     full matrix, CGEMMs on the tensor cores with FP32 emulated by BF16x9.
+//     full matrix; X and the rank-2*agg update run in the tcgen05 3xTF32
+//     kernels of tc_gemm.cu, the thin products in cuBLAS CGEMM.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <math.h>
