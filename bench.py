@@ -16,7 +16,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -100,52 +99,101 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_sample(mg=4):
-    """Oracle (numpy assembly + LAPACK zheevr from scipy's OpenBLAS, all host threads)
-    on the same deck at 9^3 plane waves (N_H = 5832), scaled to N_H = 27000 by N^3."""
+def oracle_solve(mg, n_states=8):
+    """The oracle on the benchmark deck at mg: numpy assembly + LAPACK zheevr
+    (scipy's OpenBLAS, all host threads).  Returns (seconds of assembly +
+    eigensolve, N_H, eigenvalues).  Imports no native code of this package."""
     from oracle import eigen, inputs, pipeline
     from qudos_b200 import configs
     with tempfile.TemporaryDirectory() as d:
-        configs.write_deck(d, *configs.molecule_15(mg=mg))
+        configs.write_deck(d, *configs.molecule_15(mg=mg, n_states=n_states))
         p, geo = inputs.load(d)
-        t0 = time.time()
         pr = pipeline.prepare(p, geo)
         t1 = time.time()
         H = pipeline.assemble(pr)
         lo, hi = eigen.index_window(pr.n_pw, p["N_VB"], p["N_CB"])
-        eigen.diagonalise(H, lo, hi)
+        import scipy.linalg as sla
+        w = sla.eigh(H, lower=True, subset_by_index=[lo, hi], driver="evr", overwrite_a=True, check_finite=False,
+                     eigvals_only=True)
         t2 = time.time()
-    n = pr.n_h
-    scale = (27000.0 / n) ** 3
-    return (t2 - t1) * 1e3 * scale, n, t2 - t1
+    return t2 - t1, pr.n_h, w
+
+
+def host_info():
+    model = None
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    ram = None
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemTotal"):
+                ram = round(int(ln.split()[1]) / 1024 ** 2, 1)
+                break
+    except Exception:
+        pass
+    return {"cores": os.cpu_count(), "cpu_model": model, "ram_gb": ram}
+
+
+def cpu_estimate():
+    """Bounded CPU sample for the GPU arm's cpu_baseline: the oracle at 7^3 and
+    9^3 plane waves, extrapolated to N_H = 27000 with the exponent fitted to
+    those two points (an estimate; the reference arm measures 15^3 itself)."""
+    t7, n7, _ = oracle_solve(3)
+    t9, n9, _ = oracle_solve(4)
+    p = float(np.log(t9 / t7) / np.log(n9 / n7))
+    return t9 * (27000.0 / n9) ** p * 1e3, p, (t7, n7, t9, n9)
 
 
 def run_reference(args, ws, rank):
+    """The CPU path (oracle assembly + LAPACK zheevr, all host threads) at the
+    benchmark's own size, 15^3 plane waves: one solve takes minutes, so the arm
+    runs one timed step after no warm-up and reports those counts."""
     if rank != 0:
         return
-    cores = os.cpu_count()
-    times = []
-    for i in range(args.warmup + args.steps):
-        ms, n, raw = cpu_sample()
-        if i >= args.warmup:
-            times.append(ms)
-    v = float(np.mean(times))
+    info = host_info()
+    secs, n, w = oracle_solve(args.mg)
+    v = secs * 1e3
+    fx = fixture()
+    dE = None
+    if fx is not None:
+        dE = float(np.abs(w - np.array(fx["eigenvalues_eV"])[16:48]).max()) * 1e6
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "molecule_15: two stacked InGaAs lenses, 15^3 PW, N_H=27000, 32 eigenpairs",
-                   "sample": "same deck at 9^3 PW (N_H=5832), scaled by (27000/5832)^3"},
-        "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": "oracle assembly + scipy/OpenBLAS zheevr at N_H=5832, x(27000/5832)^3"},
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": 1,
+        "warmup": 0, "ms_per_step": v, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic", "config": config_dict(n, 32, ws),
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": info["cores"], "kind": "port",
+                         "sample": "one full solve of the benchmark deck at N_H=%d: numpy assembly + "
+                                   "scipy.linalg.eigh(driver='evr', subset_by_index) on OpenBLAS" % n,
+                         "cpu_model": info["cpu_model"], "ram_gb": info["ram_gb"]},
         "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "requested_steps": args.steps, "requested_warmup": args.warmup,
+        "max_dE_ueV_vs_fixture": dE,
     }
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes per launch of xprod_kernel over its algorithmic bytes, from the ncu
-# capture summarised in profiles/xprod_kernel_9cubed.md (one launch, m = 5480).
-XPROD_TRAFFIC_RATIO = 1.083
+def fixture():
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "molecule_15", "oracle.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def config_dict(n, m, ws):
+    return {"workload": "molecule_15: two stacked InGaAs lenses, 15^3 PW, N_H=%d, %d eigenpairs" % (n, m),
+            "n_h": n, "eigenpairs": m, "parallelism": "replicas" if ws > 1 else "single",
+            "l2": "inputs larger than L2 (H is %.1f GB)" % (n * n * 16 / 1e9)}
+
+
+# DRAM bytes per launch of xprod_kernel over its algorithmic bytes (8 m^2), from
+# one ncu capture of a single launch; scaled to every launch of the step.
+XPROD_TRAFFIC = {"ratio": 1.083, "source": "ncu dram__bytes_read+write of one launch at m = 5480, scaled by 8 m^2"}
 
 
 def tc_stats(L, which):
@@ -155,10 +203,22 @@ def tc_stats(L, which):
     return n.value, ms.value, work.value
 
 
+def kramers_angles(v, vr):
+    """Largest principal angle between each consecutive column pair's span."""
+    out = []
+    for k in range(0, v.shape[1] - 1, 2):
+        qa, _ = np.linalg.qr(v[:, k:k + 2])
+        qb, _ = np.linalg.qr(vr[:, k:k + 2])
+        s = np.linalg.svd(qa.conj().T @ qb, compute_uv=False)
+        out.append(float(np.arccos(np.clip(s.min(), -1.0, 1.0))))
+    return out
+
+
 def run_gpu(args, ws, rank, local):
     import ctypes as C
     import qudos_b200 as q
     from qudos_b200 import configs, lib as L
+    from qudos_b200.pwem import last_error_bounds
     if ws > 1:
         L.check(L.lib.qd_set_device(local))
     hbm_peak, bf16_peak, peak_src = peaks()
@@ -183,9 +243,7 @@ def run_gpu(args, ws, rank, local):
         L.check(L.lib.qd_eigh_window_dev(n, H.ptr, n, lo, hi, prec, W.ptr, Z.ptr, n, None))
 
     # FP64 comparator
-    for _ in range(1):
-        step(q.QD_PREC_FP64)
-    w64 = np.empty(M)
+    step(q.QD_PREC_FP64)
     barrier(ws)
     L.check(L.lib.qd_device_synchronize())
     e0.record()
@@ -194,7 +252,10 @@ def run_gpu(args, ws, rank, local):
     e1.record()
     ms64 = allreduce_max(e0.elapsed_ms(e1) / args.fp64_steps, ws)
     t64 = L.last_timings()
+    w64 = np.empty(M)
+    v64 = np.empty((n, M), dtype=np.complex128, order="F")
     W.download(w64)
+    Z.download(v64)
     # mixed path: warm-up, then the timed steps
     for _ in range(args.warmup):
         step(q.QD_PREC_MIXED)
@@ -214,9 +275,19 @@ def run_gpu(args, ws, rank, local):
     f_n, f_ms, f_flops = tc_stats(L, 1)
     ms = allreduce_max(ms, ws)
     tmx = L.last_timings()
+    res_mx, bound_mx = last_error_bounds()
     wmx = np.empty(M)
+    vmx = np.empty((n, M), dtype=np.complex128, order="F")
     W.download(wmx)
-    dE = float(np.abs(wmx - w64).max()) * 1e6
+    Z.download(vmx)
+    dE = np.abs(wmx - w64) * 1e6
+    angles = kramers_angles(vmx, v64)
+    fx = fixture()
+    dE_or64 = dE_ormx = None
+    if fx is not None and len(fx["eigenvalues_eV"]) == 64 and M == 32:
+        wr = np.array(fx["eigenvalues_eV"])[16:48]
+        dE_or64 = (np.abs(w64 - wr) * 1e6).tolist()
+        dE_ormx = (np.abs(wmx - wr) * 1e6).tolist()
     # assembly kernel alone (HBM roofline): lower triangle, complex128
     ea0.record()
     for _ in range(3):
@@ -226,23 +297,30 @@ def run_gpu(args, ws, rank, local):
     asm_bytes = 16.0 * n * (n + 1) / 2
     # stage-1 reduction (tensor-bound): LAPACK flop count of the dense->band reduction
     flops_stage1 = 16.0 / 3.0 * n ** 3
-    st1_ms = tmx[1]
+    H.free()
     # e2e through the reference-named C-ABI with host buffers (eigenstates)
     e2e_ms, h2d, d2h = e2e_reference_call(pr, args, L)
     cpu = None
     if rank == 0 and not args.no_cpu:
-        cms, cn, raw = cpu_sample()
-        cpu = {"value": cms, "unit": "ms", "cores": os.cpu_count(), "kind": "port",
-               "sample": "oracle assembly + scipy/OpenBLAS zheevr at N_H=%d (%.1f s), x(27000/%d)^3" % (cn, raw, cn)}
+        cms, pexp, (t7, n7, t9, n9) = cpu_estimate()
+        info = host_info()
+        cpu = {"value": cms, "unit": "ms", "cores": info["cores"], "kind": "port", "estimated": True,
+               "sample": "oracle assembly + scipy/OpenBLAS zheevr on the same deck at N_H=%d (%.2f s) and N_H=%d "
+                         "(%.2f s), extrapolated to N_H=27000 with the fitted exponent %.2f; the reference arm "
+                         "times N_H=27000 itself" % (n7, t7, n9, t9, pexp),
+               "cpu_model": info["cpu_model"], "ram_gb": info["ram_gb"]}
     value = ms  # per replica; every rank solves its own instance
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128",
-        "data": "synthetic",
-        "config": {"workload": "molecule_15: two stacked InGaAs lenses, 15^3 PW, N_H=27000, 32 eigenpairs",
-                   "n_h": n, "eigenpairs": M, "parallelism": "replicas" if ws > 1 else "single",
-                   "l2": "inputs larger than L2 (H is %.1f GB)" % (n * n * 16 / 1e9)},
-        "fp64_ms_per_solve": ms64, "speedup_vs_fp64": ms64 / ms, "max_dE_ueV_vs_fp64": dE,
+        "data": "synthetic", "config": config_dict(n, M, ws),
+        "fp64_ms_per_solve": ms64, "speedup_vs_fp64": ms64 / ms, "max_dE_ueV_vs_fp64": float(dE.max()),
+        "max_dE_ueV_vs_oracle": {"fp64": max(dE_or64) if dE_or64 else None,
+                                 "mixed": max(dE_ormx) if dE_ormx else None},
+        "per_state": {"dE_ueV_mixed_vs_fp64": dE.tolist(), "dE_ueV_fp64_vs_oracle": dE_or64,
+                      "dE_ueV_mixed_vs_oracle": dE_ormx, "kramers_angle_rad_mixed_vs_fp64": angles,
+                      "residual_eV_mixed": res_mx.tolist(), "error_bound_eV_mixed": bound_mx.tolist(),
+                      "oracle": "tests/golden/molecule_15/oracle.json (LAPACK zheevr, 64-state window)"},
         "stages_ms_mixed": {"band_reduction": tmx[1], "bulge_chasing": tmx[2], "bisection": tmx[3],
                             "inverse_iteration": tmx[4], "back_transform": tmx[5], "rayleigh_ritz": tmx[6]},
         "stages_ms_fp64": {"band_reduction": t64[1], "bulge_chasing": t64[2], "bisection": t64[3],
@@ -251,10 +329,10 @@ def run_gpu(args, ws, rank, local):
         "roofline": {"bound": "hbm", "kernel": "xprod_kernel (X = A22 VT, tcgen05 3xTF32)",
                      "achieved": x_bytes / (x_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": x_bytes / (x_ms * 1e-3) / 1e9 / hbm_peak,
-                     "traffic": XPROD_TRAFFIC_RATIO * x_bytes / max(x_n, 1),
+                     "traffic": XPROD_TRAFFIC.get("ratio", 0.0) * x_bytes / max(x_n, 1) if XPROD_TRAFFIC else None,
+                     "traffic_source": XPROD_TRAFFIC.get("source") if XPROD_TRAFFIC else None,
                      "launches_per_step": x_n / args.steps, "ms_per_step": x_ms / args.steps,
-                     "note": "work = 8 m^2 bytes per launch (trailing matrix read once); peak = %s HBM copy; "
-                             "traffic = dram bytes per launch scaled from one ncu capture" % peak_src},
+                     "note": "work = 8 m^2 bytes per launch (trailing matrix read once); peak = %s HBM copy" % peak_src},
         "roofline_flush": {"bound": "tensor", "kernel": "flush_kernel (Hermitian rank-2K update, tcgen05 3xTF32)",
                            "achieved": f_flops / (f_ms * 1e-3) / 1e12, "peak": tf32_peak / 3.0, "unit": "TFLOP/s",
                            "frac": f_flops / (f_ms * 1e-3) / 1e12 / (tf32_peak / 3.0), "traffic": None,
@@ -279,77 +357,25 @@ def run_gpu(args, ws, rank, local):
 
 
 def e2e_reference_call(pr, args, L):
-    """eigenstates() (the reference's routine) with the tables in host memory,
-    H assembled on the device, eigenvectors copied back: timed on the host."""
-    import ctypes as C
-    from qudos_b200 import pwem
+    """eigenstates() (the reference's routine) with the coefficient tables in
+    host memory and the eigenvectors copied back to the caller's host buffers,
+    as the reference's main program calls it; mean host wall time of the timed
+    calls after one warm-up call."""
+    from qudos_b200.refabi import ReferenceCall
     os.environ["QD_PRECISION"] = "mixed"
+    call = ReferenceCall.from_problem(pr)
+    call.eigenstates(pr.n_vb, pr.n_cb)
+    reps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        call.eigenstates(pr.n_vb, pr.n_cb)
+    ms = (time.perf_counter() - t0) * 1e3 / reps
+    nT = len(call._chi[1])
     ns = pr.n_shape
-    shp = None
-    geo = pr.geometry(ns)
-    mat = pr.materials(ns)
-    n_pw = pr.n_pw
-    N = round(n_pw ** (1.0 / 3.0))
-    NT = 2 * N - 1
-    shp = (NT, NT, NT)
-    nT = NT ** 3
-    chi = [None] + [pr.table(0, s, 0, shp) for s in range(1, ns)]
-    eps = [pr.table(1, c, 0, shp) for c in range(6)]
-    phi = pr.table(2, 0, 0, shp)
-    conv = [None] + [[pr.table(3, s, c, shp) for c in range(8)] for s in range(1, ns)]
-    keep = []
-
-    class CF(C.Structure):
-        _fields_ = [("chi", C.c_void_p)]
-
-    class ST(C.Structure):
-        _fields_ = [(k, C.c_void_p) for k in ("xx", "yy", "zz", "yz", "xz", "xy")]
-
-    class CV(C.Structure):
-        _fields_ = [(k, C.c_void_p) for k in ("char_xx", "char_yy", "char_zz", "char_yz", "char_xz", "char_xy",
-                                              "char_hydrostatic", "char_biaxial")] + [("rest%d" % i, C.c_void_p)
-                                                                                       for i in range(24)]
-    cf = (CF * ns)()
-    for s in range(1, ns):
-        cf[s].chi = chi[s].ctypes.data
-    cv = (CV * ns)()
-    for s in range(1, ns):
-        for c, k in enumerate(("char_xx", "char_yy", "char_zz", "char_yz", "char_xz", "char_xy", "char_hydrostatic",
-                               "char_biaxial")):
-            setattr(cv[s], k, conv[s][c].ctypes.data)
-    st = ST(*[e.ctypes.data for e in eps])
-    C.c_void_p.in_dll(L.lib, "characteristic_function_G").value = C.addressof(cf)
-    C.c_void_p.in_dll(L.lib, "convolutions_char_strain").value = C.addressof(cv)
-    C.memmove(C.addressof(ST.in_dll(L.lib, "strain_G")), C.addressof(st), C.sizeof(ST))
-    C.c_void_p.in_dll(L.lib, "phi_piezo_G").value = phi.ctypes.data
-    C.c_int.in_dll(L.lib, "include_strain").value = 1
-    C.c_int.in_dll(L.lib, "include_piezo").value = 1
-    C.c_int64.in_dll(L.lib, "N_H").value = pr.n_h
-    C.c_int64.in_dll(L.lib, "na_rows").value = pr.n_h
-    grids = [np.ascontiguousarray(((2 * np.pi) / L_) * (0.5 * (1.0 - NT) + np.arange(NT))) for L_ in
-             (geo[0]["L1"], geo[0]["L2"], geo[0]["L3"])]
-    basis = L.WaveVectors(N, N, N, NT, NT, NT, *[g.ctypes.data_as(C.POINTER(C.c_double)) for g in grids], 0.0, 0.0,
-                          0.0)
-    gstruct = (L.SupercellGeometry * ns)(*[L.SupercellGeometry(**g) for g in geo])
-    mstruct = (L.MaterialParams * ns)(*[L.MaterialParams(**m) for m in mat])
-    nstates = (C.c_int * 2)(pr.n_vb, pr.n_cb)
-    vb = (L.Eigenstate * (2 * pr.n_vb))()
-    cb = (L.Eigenstate * (2 * pr.n_cb))()
-    bufs = [np.zeros(pr.n_h, dtype=np.complex128) for _ in range(2 * pr.n_vb + 2 * pr.n_cb)]
-    for i in range(2 * pr.n_vb):
-        vb[i].fourier = bufs[i].ctypes.data
-    for i in range(2 * pr.n_cb):
-        cb[i].fourier = bufs[2 * pr.n_vb + i].ctypes.data
-    F = L.Vector(0.0, 0.0, 0.0)
-    times = []
-    for i in range(2):
-        t0 = time.perf_counter()
-        L.lib.eigenstates(ns, nstates, F, basis, gstruct, mstruct, vb, cb)
-        times.append(time.perf_counter() - t0)
     h2d = 16 * nT * ((ns - 1) + 6 + 1 + 8 * (ns - 1))
-    d2h = 16 * pr.n_h * len(bufs) + 8 * len(bufs)
-    keep.append((cf, cv, st, grids, bufs))
-    return times[-1] * 1e3, h2d, d2h
+    M = 2 * pr.n_vb + 2 * pr.n_cb
+    d2h = 16 * pr.n_h * M + 8 * M
+    return ms, h2d, d2h
 
 
 def main():
@@ -363,17 +389,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
-    if args.impl == "gpu":
-        import qudos_b200  # noqa: F401  (before torch: the toolkit cuBLAS must be the one loaded)
+    if args.impl == "reference":
+        # rank 0 alone runs the CPU path; the other ranks have nothing to do
+        run_reference(args, ws, rank)
+        return
+    import qudos_b200.lib  # noqa: F401  (before torch: the toolkit cuBLAS must be the one loaded)
     if ws > 1:
         import torch.distributed as dist
         import datetime
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.impl == "reference":
-            run_reference(args, ws, rank)
-        else:
-            run_gpu(args, ws, rank, local)
+        run_gpu(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -126,9 +126,14 @@ void eigenstates(int N_shape, int *N_states, struct vector F, struct wave_vector
                  struct supercell_geometry *supercell, struct material_params *parameters,
                  struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb);
 
-/* Replaces code/source/8_band/coulomb_matrix_elements.c:24 for include_CME = 1
- * (no multipole corrections) and a Coulomb cell equal to the electronic
- * structure cell.  CME arrays are allocated by the caller with the sizes of
+/* Replaces code/source/8_band/coulomb_matrix_elements.c:24.  include_CME 1-4
+ * (1: the Fourier-space integrals only; 2: plus the Madelung monopole term;
+ * 3: plus dipole; 4: plus quadrupole, coulomb_matrix_elements.c:250-557), a
+ * free Coulomb cell (coulomb_region_type 0) equal to or larger than the
+ * electronic-structure cell, with coulomb_basis.N_G* plane waves per axis.
+ * The real-space Madelung sum follows the reference's split over the
+ * `nprocs` global.  Commensurate cells (coulomb_region_type 1) print an error
+ * and exit.  CME arrays are allocated by the caller with the sizes of
  * 8_band_main.c:1752-1775. */
 void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coulomb_basis,
                              struct supercell_geometry *supercell,
@@ -231,6 +236,19 @@ int qd_event_destroy(void *ev);
  * memory pool between calls; this returns the cached memory to the driver. */
 int qd_trim_pool(void);
 
+/* Limits of the library's bounded device-side waits, for the current device
+ * (a negative value restores that limit's default):
+ *   barrier_polls  polls of the panel factorisation's grid barrier (default
+ *                  2^26, about three seconds);
+ *   sweep_polls    polls of a bulge-chasing sweep waiting on the previous one
+ *                  (default 2^25);
+ *   pipeline_ns    nanoseconds a tensor-core kernel's pipeline stage waits
+ *                  (default 2e9).
+ * A wait that runs out makes the call return QD_ERR_TIMEOUT; the kernels exit
+ * cleanly and the device stays usable.  Waits that drain a kernel's own copies
+ * in flight before it exits keep a fixed 2 s bound. */
+int qd_set_wait_limits(long long barrier_polls, long long sweep_polls, long long pipeline_ns);
+
 /* Stage timings of the last qd_problem_solve / qd_eigh_window_dev call (ms):
  * [0] assembly, [1] band reduction, [2] bulge chasing, [3] bisection,
  * [4] inverse iteration, [5] back-transform, [6] refinement. */
@@ -308,20 +326,53 @@ int qd_tc_kernel_stats(int which, long long *launches, double *ms, double *work)
  * elsewhere. */
 int qd_gemm_peak(int kind, int n, int reps, double *tflops);
 
+/* FP64 building blocks of the solver's last stage, exposed for checking
+ * (device pointers, column-major complex128):
+ *   qd_hemm_lower_dev   Y = H X + beta Y, H Hermitian n x n with its lower
+ *                       triangle stored (the reference's layout), X n x k;
+ *   qd_gram_dev         C = A^H B (ka x kb) reduced over n rows;
+ *   qd_zgemm_small_dev  Y = Z C + beta Y, C small (k x k2);
+ *   qd_residual_norms_dev  res[j] = ||R[:, j] - w[j] Z[:, j]||. */
+int qd_hemm_lower_dev(int64_t n, const void *H, int64_t ld, const void *X, int64_t ldx, int k, void *Y, int64_t ldy,
+                      double beta, void *stream);
+int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb, void *C, int ldc,
+                void *stream);
+int qd_zgemm_small_dev(int64_t n, const void *Z, int64_t ldz, int k, const void *C, int ldc, int k2, void *Y,
+                       int64_t ldy, double beta, void *stream);
+int qd_residual_norms_dev(int64_t n, const void *R, int64_t ldr, const void *Z, int64_t ldz, const double *w_dev,
+                          int m, double *res_dev, void *stream);
+
+/* Residual check of host eigenpairs (m values, N_H x m vectors) of a loaded
+ * problem against its H, assembled on the device in FP64:
+ * res[j] = ||H z_j - w_j z_j|| (eV), *orth = max |(Z^H Z - I)_ij|,
+ * *hnorm = max |H_ij|. */
+int qd_problem_residuals(qd_problem *pr, int m, const double *eigval, const void *eigvec, double *res, double *orth,
+                         double *hnorm);
+
+/* Error bounds of the last mixed-precision solve on the calling thread, per
+ * window state: residual[i] = ||H x_i - theta_i x_i|| in FP64 and
+ * bound[i] = ||r||^2 / delta (Kato-Temple), delta the distance from theta_i to
+ * the nearest Ritz value outside its degenerate group.  The mixed solve
+ * returns QD_ERR_CONVERGENCE when a bound exceeds QD_BOUND_TOL (eV, default
+ * 1e-6).  Returns the number of states (either pointer may be NULL). */
+int qd_last_error_bounds(double *residual, double *bound, int n);
+
 /* Allocation-free eigenvalues of a Hermitian tridiagonal matrix for the index
  * window [lo, hi] (0-based, ascending), by the same Sturm-count multisection
- * as the solver's bisection stage.  No reference counterpart: it serves
- * callers that may not allocate device memory (code running inside a stream
- * capture, or under a caller-owned memory budget).
+ * as the solver's bisection stage.  No reference counterpart: it is for
+ * callers that cannot call cudaMalloc, such as a host program whose device
+ * memory belongs to another allocator (a framework's caching pool, a fixed
+ * per-process budget) and which hands this library only its own buffers.
  *   AB: device, band storage with ldb >= 2; AB[j*ldb] is the diagonal entry
  *       (real part used), AB[1 + j*ldb] the sub-diagonal entry (j, j+1).
  *   w:  device, hi - lo + 1 doubles.
- * Scratch is file-scope device memory for n <= QD_STATIC_TRI_MAX rows; larger
- * n returns QD_ERR_ARG.  The scratch is shared by all calls on a device, so
- * calls that may overlap (several streams or host threads) must be
+ * Scratch is a file-scope device array for n <= QD_STATIC_TRI_MAX rows
+ * (1 MB, held by every GPU that loads the library until exit); larger n
+ * returns QD_ERR_ARG.  Every call on a device shares that scratch, so calls
+ * that overlap on the GPU (several streams or host threads) race and must be
  * serialised by the caller.  The first call on each device resolves the
- * scratch addresses (cudaGetSymbolAddress); make that first call outside any
- * stream capture. */
+ * scratch address (cudaGetSymbolAddress, with that device current); make that
+ * first call before any stream capture. */
 #define QD_STATIC_TRI_MAX 65536
 int qd_tridiag_eigvals_noalloc(const void *AB, int ldb, int n, int lo, int hi, double *w, void *stream);
 

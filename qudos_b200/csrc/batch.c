@@ -77,9 +77,12 @@ int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, d
     qsort_r(q.order, (size_t)n, sizeof(int), by_size_desc, problems);
     cudaGetDevice(&q.device);
     pthread_mutex_init(&q.mu, NULL);
+    /* handles of the threads that did start are kept contiguous, so only those are joined */
     int started = 0;
-    for (int t = 0; t < n_threads; t++)
-        if (pthread_create(&th[t], NULL, batch_worker, &q) == 0) started++;
+    for (int t = 0; t < n_threads; t++) {
+        pthread_t tid;
+        if (pthread_create(&tid, NULL, batch_worker, &q) == 0) th[started++] = tid;
+    }
     if (started == 0) batch_worker(&q); /* no threads available: run in the caller */
     for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
     pthread_mutex_destroy(&q.mu);

@@ -37,6 +37,14 @@ extern "C" int qd_band_invit(const double2 *AB0, int ldb, int n, int b, const do
                              const int *gstart_dev, const int *gsize_dev, double2 *Lw, double2 *Uw, int *ipivw,
                              double2 *Z, int64_t ldz, double bnorm, double2 *ywork, void *stream);
 extern "C" cublasHandle_t qd_cublas(void);
+extern "C" int qd_hemm_lower_dev(int64_t n, const void *H, int64_t ld, const void *X, int64_t ldx, int k, void *Y,
+                                 int64_t ldy, double beta, void *stream);
+extern "C" int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb, void *C,
+                           int ldc, void *stream);
+extern "C" int qd_zgemm_small_dev(int64_t n, const void *Z, int64_t ldz, int k, const void *Cm, int ldc, int k2,
+                                  void *Y, int64_t ldy, double beta, void *stream);
+extern "C" int qd_residual_norms_dev(int64_t n, const void *R, int64_t ldr, const void *Z, int64_t ldz,
+                                     const double *w_dev, int m, double *res_dev, void *stream);
 
 static thread_local double g_timings[8];  // per host thread (concurrent batched solves)
 extern "C" int qd_last_timings(double *ms, int n) {
@@ -310,6 +318,61 @@ static int block_size_default() {
     return b;
 }
 
+// Per-state error bounds of the last mixed-precision solve (eV): the FP64
+// residual norm ||H x - theta x|| of each window state and the Kato-Temple
+// bound ||r||^2 / delta on |lambda - theta|, delta being the distance from
+// theta to the nearest Ritz value outside its degenerate group (the guard
+// states supply the neighbours of the window's edges).
+static thread_local std::vector<double> g_res, g_bound;
+
+extern "C" int qd_last_error_bounds(double *residual, double *bound, int n) {
+    for (int i = 0; i < n && i < (int)g_res.size(); i++) {
+        if (residual) residual[i] = g_res[i];
+        if (bound) bound[i] = g_bound[i];
+    }
+    return (int)g_res.size();
+}
+
+// Largest bound accepted before the solve reports QD_ERR_CONVERGENCE (eV).
+static double bound_tolerance(void) {
+    const char *s = getenv("QD_BOUND_TOL");
+    return s ? atof(s) : 1.0e-6;
+}
+
+static int window_error_bounds(const double *theta, int k, int off, int M, const double *res, int guard_below,
+                               int guard_above) {
+    g_res.assign(res, res + M);
+    g_bound.assign(M, 0.0);
+    double worst = 0.0;
+    int iw = -1;
+    for (int i = 0; i < M; i++) {
+        const double t = theta[off + i];
+        const double deg = 1e-9 * (fabs(t) > 1.0 ? fabs(t) : 1.0);
+        double delta = INFINITY;
+        for (int j = 0; j < k; j++)
+            if (fabs(theta[j] - t) > deg && fabs(theta[j] - t) < delta) delta = fabs(theta[j] - t);
+        // an edge state with no Ritz value beyond it in the basis has no neighbour there to bound against
+        const bool edge_lo = off + i == 0 && guard_below, edge_hi = off + i == k - 1 && guard_above;
+        double b = (edge_lo || edge_hi || !isfinite(delta)) ? INFINITY : res[i] * res[i] / delta;
+        // the degenerate group's residual is the root sum of squares of its members'
+        double rg = 0.0;
+        for (int j = 0; j < M; j++)
+            if (fabs(theta[off + j] - t) <= deg) rg += res[j] * res[j];
+        if (isfinite(b)) b = rg / delta;
+        g_bound[i] = b;
+        if (!(b <= worst)) {
+            worst = b;
+            iw = i;
+        }
+    }
+    if (!(worst <= bound_tolerance()))
+        return qd_set_error(QD_ERR_CONVERGENCE,
+                            "mixed-precision refinement: error bound %.3g eV of window state %d above %.3g eV "
+                            "(residual %.3g eV); raise QD_GUARD",
+                            worst, iw, bound_tolerance(), iw >= 0 ? res[iw] : 0.0);
+    return QD_OK;
+}
+
 extern "C" int qd_mixed_guard(void) {
     const char *s = getenv("QD_GUARD");
     return s ? atoi(s) : 8;
@@ -326,6 +389,8 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     int g = mixed ? qd_mixed_guard() : 0;
     int lo2 = lo - g < 0 ? 0 : lo - g, hi2 = hi + g > n - 1 ? (int)n - 1 : hi + g;
     int k = hi2 - lo2 + 1, M = hi - lo + 1;
+    if (mixed && k > 128)
+        return qd_set_error(QD_ERR_UNSUPPORTED, "mixed precision: window plus guard states above 128 (%d)", k);
     int ldb = 2 * b + 1;
     Timer tm(st);
     tm.mark();  // 0
@@ -420,40 +485,47 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
         CUDA_OK(cudaGetLastError());
         tm.mark();  // 5
         // ---- FP64 Rayleigh-Ritz against H (lower triangle, complex128)
-        cublasHandle_t h = qd_cublas();
-        BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
-        double2 *Y, *S, *Ak, *C, *Xn;
-        double *theta;
+        double2 *Y, *S, *Ak, *C, *Xn, *YC;
+        double *theta, *res;
         int *info;
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Y, sizeof(double2) * n * k, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Xn, sizeof(double2) * n * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&YC, sizeof(double2) * n * M, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&S, sizeof(double2) * k * k, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&Ak, sizeof(double2) * k * k, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&C, sizeof(double2) * k * k, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&theta, sizeof(double) * k, st));
+        CUDA_OK((cudaError_t)qd_pool_alloc((void **)&res, sizeof(double) * M, st));
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&info, sizeof(int), st));
         CUDA_OK(cudaMemsetAsync(info, 0, sizeof(int), st));
-        const cuDoubleComplex one = {1, 0}, zero = {0, 0};
-        BLAS_OK(cublasZhemm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, (int)n, k, &one, (cuDoubleComplex *)H, (int)ld,
-                            (cuDoubleComplex *)Zb, (int)n, &zero, (cuDoubleComplex *)Y, (int)n));
-        BLAS_OK(cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, k, k, (int)n, &one, (cuDoubleComplex *)Zb, (int)n,
-                            (cuDoubleComplex *)Zb, (int)n, &zero, (cuDoubleComplex *)S, k));
-        BLAS_OK(cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, k, k, (int)n, &one, (cuDoubleComplex *)Zb, (int)n,
-                            (cuDoubleComplex *)Y, (int)n, &zero, (cuDoubleComplex *)Ak, k));
+        RC(qd_hemm_lower_dev(n, H, ld, Zb, n, k, Y, n, 0.0, st));     // Y = H Z
+        RC(qd_gram_dev(n, Zb, n, k, Zb, n, k, S, k, st));               // S = Z^H Z
+        RC(qd_gram_dev(n, Zb, n, k, Y, n, k, Ak, k, st));               // A = Z^H H Z
+        qd_count_launch(1);
         small_rr_kernel<<<1, 256, 0, st>>>(k, S, Ak, C, theta, info);
         CUDA_OK(cudaGetLastError());
-        BLAS_OK(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, k, k, &one, (cuDoubleComplex *)Zb, (int)n,
-                            (cuDoubleComplex *)C, k, &zero, (cuDoubleComplex *)Xn, (int)n));
-        int off = lo - lo2;
+        RC(qd_zgemm_small_dev(n, Zb, n, k, C, k, k, Xn, n, 0.0, st));   // X = Z C
+        // residuals of the window's Ritz pairs: H X - X Theta = (H Z) C - X Theta
+        const int off = lo - lo2;
+        RC(qd_zgemm_small_dev(n, Y, n, k, C + (int64_t)off * k, k, M, YC, n, 0.0, st));
+        RC(qd_residual_norms_dev(n, YC, n, Xn + (int64_t)off * n, n, theta + off, M, res, st));
         CUDA_OK(cudaMemcpy2DAsync(Z_dev, sizeof(double2) * ldz, Xn + (int64_t)off * n, sizeof(double2) * n,
                                   sizeof(double2) * n, M, cudaMemcpyDeviceToDevice, st));
         CUDA_OK(cudaMemcpyAsync(w_dev, theta + off, sizeof(double) * M, cudaMemcpyDeviceToDevice, st));
         int hinfo = 0;
+        std::vector<double> th_h(k), res_h(M);
         CUDA_OK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(th_h.data(), theta, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(res_h.data(), res, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
         tm.mark();  // 6
         CUDA_OK(cudaStreamSynchronize(st));
-        void *rr_bufs[] = {Y, Xn, S, Ak, C, theta, info, Z32};
+        void *rr_bufs[] = {Y, Xn, YC, S, Ak, C, theta, res, info, Z32};
         for (void *p : rr_bufs) qd_pool_free(p, st);
+        if (!hinfo) {
+            int brc = window_error_bounds(th_h.data(), k, off, M, res_h.data(), lo2 > 0 || off > 0,
+                                          hi2 < n - 1 || off + M < k);
+            if (brc) return brc;
+        }
         if (hinfo) return qd_set_error(QD_ERR_CONVERGENCE, "Rayleigh-Ritz: Gram matrix not positive definite");
     }
     CUDA_OK(cudaStreamSynchronize(st));

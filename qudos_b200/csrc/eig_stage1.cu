@@ -34,7 +34,10 @@
 #include "eig_common.cuh"
 #include "qd_internal.h"
 
-#define QD_BAR_LIMIT (1LL << 26)
+// Polls before a panel's grid-barrier wait gives up (set at run time by
+// qd_set_wait_limits; the default is about three seconds of polling).
+#define QD_BAR_LIMIT_DEFAULT (1LL << 26)
+__device__ long long g_bar_limit = QD_BAR_LIMIT_DEFAULT;
 
 // ---------------------------------------------------------------------------
 // panel QR
@@ -89,8 +92,9 @@ __device__ __forceinline__ bool grid_arrive_wait(unsigned *ctr, unsigned target,
         ok = 1;
         asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
         long long it = 0;
+        const long long limit = g_bar_limit;
         while (ld_acquire_u32(ctr) < target) {
-            if (++it > QD_BAR_LIMIT || *(volatile int *)err) {
+            if (++it > limit || *(volatile int *)err) {
                 atomicExch(err, 6);
                 ok = 0;
                 break;
@@ -307,6 +311,12 @@ __global__ void form_t_kernel(const cpx<R> *gram, int ldg, const cpx<R> *tau, cp
         int rc_ = (x);                \
         if (rc_ != QD_OK) return rc_; \
     } while (0)
+
+extern "C" int qd_stage1_set_wait_limit(long long polls) {
+    const long long v = polls < 0 ? QD_BAR_LIMIT_DEFAULT : polls;
+    CUDA_OK(cudaMemcpyToSymbol(g_bar_limit, &v, sizeof(v)));
+    return QD_OK;
+}
 
 static int n_panels(int64_t n, int b) {
     int c = 0;

@@ -29,7 +29,10 @@
 
 typedef cpx<double> zd;
 
-#define SPIN_LIMIT (1LL << 25)
+// Polls before a wait on the previous sweep gives up (set at run time by
+// qd_set_wait_limits; the default is about a second and a half of polling).
+#define QD_SPIN_LIMIT_DEFAULT (1LL << 25)
+__device__ long long g_spin_limit = QD_SPIN_LIMIT_DEFAULT;
 #define PROGRESS_DONE 0x7fffffff
 #define QD_INVIT_ITERS 2
 
@@ -55,8 +58,9 @@ __device__ bool wait_progress(const int *progress, int s_prev, int need, int *er
     if (threadIdx.x == 0) {
         ok = 1;
         long long it = 0;
+        const long long limit = g_spin_limit;
         while (ld_acquire(progress + s_prev) < need) {
-            if (++it > SPIN_LIMIT || *(volatile int *)err) {
+            if (++it > limit || *(volatile int *)err) {
                 atomicExch(err, QD_ERR_TIMEOUT);
                 ok = 0;
                 break;
@@ -575,6 +579,12 @@ __global__ void __launch_bounds__(256) band_invit_kernel(const double2 *AB, int 
             return qd_set_error(QD_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
     } while (0)
 
+extern "C" int qd_stage2_set_wait_limit(long long polls) {
+    const long long v = polls < 0 ? QD_SPIN_LIMIT_DEFAULT : polls;
+    CUDA_OK(cudaMemcpyToSymbol(g_spin_limit, &v, sizeof(v)));
+    return QD_OK;
+}
+
 extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *err, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     int dev, nsm, per_sm = 0;
@@ -650,24 +660,29 @@ extern "C" int qd_tridiag_eigvals_noalloc(const void *ABv, int ldb, int n, int l
     if (dev < 0 || dev >= QD_STATIC_MAX_DEVICES)
         return qd_set_error(QD_ERR_ARG, "qd_tridiag_eigvals_noalloc: device %d not supported", dev);
     double **a = g_static_addr[dev];
-    if (!a[0]) {  // first call on this device: resolve the scratch addresses once
+    double *d0 = __atomic_load_n(&a[0], __ATOMIC_ACQUIRE);
+    if (!d0) {  // first call on this device: resolve the scratch addresses once
         void *p0 = nullptr, *p1 = nullptr, *p2 = nullptr;
         CUDA_OK(cudaGetSymbolAddress(&p0, g_static_tri_d));
         CUDA_OK(cudaGetSymbolAddress(&p1, g_static_tri_e2));
         CUDA_OK(cudaGetSymbolAddress(&p2, g_static_tri_bounds));
-        a[1] = (double *)p1;
-        a[2] = (double *)p2;
-        a[0] = (double *)p0;
+        // a[1] and a[2] are published by the release store of a[0]; a thread
+        // that sees a[0] through the acquire load above also sees them
+        __atomic_store_n(&a[1], (double *)p1, __ATOMIC_RELAXED);
+        __atomic_store_n(&a[2], (double *)p2, __ATOMIC_RELAXED);
+        __atomic_store_n(&a[0], (double *)p0, __ATOMIC_RELEASE);
+        d0 = (double *)p0;
     }
+    double *e2s = __atomic_load_n(&a[1], __ATOMIC_RELAXED), *bnds = __atomic_load_n(&a[2], __ATOMIC_RELAXED);
     // Every scratch element that is read is written first in the same call
     // (d and e2 for the n rows by tri_extract_kernel, the bounds by
     // gersh_kernel), so nothing needs clearing.
     cudaStream_t st = (cudaStream_t)stream;
     qd_count_launch(3);
-    tri_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(AB, ldb, n, a[0], a[1]);
-    gersh_kernel<<<1, 1024, 0, st>>>(a[0], a[1], n, a[2]);
+    tri_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(AB, ldb, n, d0, e2s);
+    gersh_kernel<<<1, 1024, 0, st>>>(d0, e2s, n, bnds);
     int m = hi - lo + 1;
-    bisect_kernel<<<(m * 32 + 127) / 128, 128, 0, st>>>(a[0], a[1], n, lo, hi, a[2], w);
+    bisect_kernel<<<(m * 32 + 127) / 128, 128, 0, st>>>(d0, e2s, n, lo, hi, bnds, w);
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }

@@ -61,6 +61,17 @@ static long long g_launches = 0;
 void qd_count_launch(int n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
 long long qd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
+int qd_stage1_set_wait_limit(long long polls);
+int qd_stage2_set_wait_limit(long long polls);
+int qd_tc_set_wait_limit(long long ns);
+
+int qd_set_wait_limits(long long barrier_polls, long long sweep_polls, long long pipeline_ns) {
+    int rc = qd_stage1_set_wait_limit(barrier_polls);
+    if (rc == QD_OK) rc = qd_stage2_set_wait_limit(sweep_polls);
+    if (rc == QD_OK) rc = qd_tc_set_wait_limit(pipeline_ns);
+    return rc;
+}
+
 /* Stream-ordered pool allocations of the solve path.  The first use on a
  * device raises the release threshold of its default pool so that freed
  * workspace stays mapped for the next solve; qd_trim_pool() hands it back. */

@@ -52,7 +52,13 @@ namespace {
 
 constexpr int BKF = 32;  // floats per k-block row: 128 bytes = one SWIZZLE_128B atom
 constexpr int TILE_M = 128;
-constexpr unsigned long long WAIT_NS = 2000000000ull;
+// A pipeline wait gives up after g_wait_ns of %globaltimer (set at run time by
+// qd_set_wait_limits, default 2 s).  The waits that drain a CTA's own copies
+// and MMAs in flight before it exits keep the fixed DRAIN_NS, so that an
+// aborted CTA never leaves with work still landing in its shared memory.
+constexpr unsigned long long WAIT_NS_DEFAULT = 2000000000ull;
+constexpr unsigned long long DRAIN_NS = 2000000000ull;
+__device__ unsigned long long g_wait_ns = WAIT_NS_DEFAULT;
 
 struct TcArgs {
     int n_items, tiles_m, tiles_n, splits, kblocks;
@@ -93,18 +99,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait on one phase.  Gives up after WAIT_NS or when another role
+// Bounded wait on one phase.  Gives up after g_wait_ns or when another role
 // has raised the CTA's abort flag; returns false then.
 // The clock and the abort flag are read every 64 polls only: the waiting warps
 // of a CTA would otherwise keep the SM's conversion/special-register pipe busy.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
     if (mbar_try(bar, parity)) return true;
-    unsigned long long t0 = now_ns();
+    const unsigned long long t0 = now_ns(), limit = g_wait_ns;
     for (uint32_t it = 1;; it++) {
         if (mbar_try(bar, parity)) return true;
         if ((it & 63) == 0) {
             if (*abort_flag) return false;
-            if (now_ns() - t0 > WAIT_NS) return false;
+            if (now_ns() - t0 > limit) return false;
         }
     }
 }
@@ -283,7 +289,7 @@ __device__ __forceinline__ void ring_prev(int &s, uint32_t &ph, int n) {
 __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity) {
     unsigned long long t0 = now_ns();
     for (uint32_t it = 1; !mbar_try(bar, parity); it++)
-        if ((it & 63) == 0 && now_ns() - t0 >= WAIT_NS) break;
+        if ((it & 63) == 0 && now_ns() - t0 >= DRAIN_NS) break;
 }
 
 // ---------------------------------------------------------------------------
@@ -968,6 +974,12 @@ int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap
 
 // Work buffers of the tensor-core path (device), sized for an n x n matrix
 // and rank-2K updates with K <= kmax.
+extern "C" int qd_tc_set_wait_limit(long long ns) {
+    const unsigned long long v = ns < 0 ? WAIT_NS_DEFAULT : (unsigned long long)ns;
+    CUDA_OK(cudaMemcpyToSymbol(g_wait_ns, &v, sizeof(v)));
+    return QD_OK;
+}
+
 extern "C" void qd_tc_work_free_on(struct QdTcWork *w, cudaStream_t st);
 
 struct QdTcWork {

@@ -108,6 +108,12 @@ _sig("qd_tc_xprod", ci, [vp, i64, i64, i64, ci, vp, i64, ci, vp, i64, vp, vp])
 _sig("qd_tc_flush", ci, [vp, i64, i64, ci, vp, vp, i64, i64, ci, vp, vp])
 _sig("qd_tc_kernel_stats", ci, [ci, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)])
 _sig("qd_gemm_peak", ci, [ci, ci, ci, C.POINTER(C.c_double)])
+_sig("qd_set_wait_limits", ci, [C.c_longlong, C.c_longlong, C.c_longlong])
+_sig("qd_hemm_lower_dev", ci, [i64, vp, i64, vp, i64, ci, vp, i64, C.c_double, vp])
+_sig("qd_gram_dev", ci, [i64, vp, i64, ci, vp, i64, ci, vp, ci, vp])
+_sig("qd_zgemm_small_dev", ci, [i64, vp, i64, ci, vp, ci, ci, vp, i64, C.c_double, vp])
+_sig("qd_problem_residuals", ci, [vp, ci, vp, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)])
+_sig("qd_last_error_bounds", ci, [vp, vp, ci])
 _sig("qd_tridiag_eigvals_noalloc", ci, [vp, ci, ci, ci, ci, vp, vp])
 _sig("qd_tridiag_bisect", ci, [vp, ci, ci, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_dev_alloc", ci, [C.c_size_t, C.POINTER(vp)])

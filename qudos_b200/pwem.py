@@ -81,6 +81,18 @@ class Problem:
         L.check(L.lib.qd_problem_solve(self._h, prec, w.ctypes.data, v.ctypes.data))
         return w, v
 
+    def residuals(self, w, v):
+        """FP64 check of eigenpairs against this problem's H, assembled on the
+        device: (||H v_j - w_j v_j|| per state in eV, max |V^H V - I|, max |H_ij|)."""
+        v = np.asfortranarray(v, dtype=np.complex128)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        m = v.shape[1]
+        res = np.zeros(m)
+        orth, hn = C.c_double(0), C.c_double(0)
+        L.check(L.lib.qd_problem_residuals(self._h, m, w.ctypes.data, v.ctypes.data, res.ctypes.data, C.byref(orth),
+                                           C.byref(hn)))
+        return res, orth.value, hn.value
+
     def coulomb(self, v, n_vb_states, n_cb_states, madelung_ranks=1):
         """Coulomb matrix elements of the states v (N_H x M, VB states first)
         with the deck's CME setting (coulomb_matrix_elements.c:24).  Returns
@@ -116,6 +128,16 @@ class Problem:
         rows = np.stack([w, 100.0 * (bl[:, 3] + bl[:, 7]), 100.0 * (bl[:, 2] + bl[:, 6]),
                          100.0 * (bl[:, 1] + bl[:, 5]), 100.0 * (bl[:, 0] + bl[:, 4])], axis=1)
         return rows[:m_vb][::-1], rows[m_vb:]
+
+
+def last_error_bounds():
+    """Per-state FP64 residual norms and Kato-Temple eigenvalue error bounds (eV)
+    of the window of the last mixed-precision solve on this host thread."""
+    n = L.lib.qd_last_error_bounds(None, None, 0)
+    res, bound = np.zeros(n), np.zeros(n)
+    if n:
+        L.lib.qd_last_error_bounds(res.ctypes.data, bound.ctypes.data, n)
+    return res, bound
 
 
 def solve_batch(problems, prec=L.QD_PREC_MIXED, n_threads=8):

@@ -1,0 +1,153 @@
+"""The measured workloads at their own sizes (GPU).
+
+* pyramid_11 (11^3 plane waves, N_H = 10648, 8 e + 8 h Kramers pairs, Fz =
+  10 kV/cm): the FP64 path against the oracle run here (numpy assembly +
+  LAPACK zheevr) within 1e-9 eV and 1e-7 rad per Kramers pair; the mixed path
+  within 1 micro-eV.  The oracle run is checked against the committed fixture
+  tests/golden/pyramid_11/oracle.json first.
+* molecule_15 (15^3, N_H = 27000, the benchmark deck) against the committed
+  oracle fixture tests/golden/molecule_15/oracle.json (made by
+  tests/golden/make_configs.py): the 64-state window (16 e + 16 h pairs) and
+  the 32-state window of the metric, FP64 and mixed.  Eigenvalues within
+  1e-9 eV (FP64) / 1 micro-eV (mixed); the gauge-invariant probe projections
+  of every Kramers pair and its Bloch characters; and an FP64 residual check
+  ||H z - lambda z|| on the device with ||Z^H Z - I||.
+Per-state errors are printed (pytest -s shows them).
+"""
+
+import json
+import os
+import tempfile
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+import qudos_b200 as q
+from oracle import eigen, inputs, pipeline
+from qudos_b200 import configs
+from qudos_b200.pwem import last_error_bounds
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _fixture(name):
+    with open(os.path.join(GOLDEN, name, "oracle.json")) as f:
+        return json.load(f)
+
+
+def _probes(n_h, fx):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mk", os.path.join(GOLDEN, "make_configs.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    return mk, mk.probe_vectors(n_h, fx["n_probes"], fx["probe_seed"])
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu():
+    assert q.device_count() > 0, "no CUDA device visible"
+
+
+def _pair_angles(v, vr):
+    return np.array([sla.subspace_angles(v[:, k:k + 2], vr[:, k:k + 2]).max() for k in range(0, v.shape[1], 2)])
+
+
+# --------------------------------------------------------------------------- C2
+@pytest.fixture(scope="module")
+def pyramid(tmp_path_factory):
+    d = str(tmp_path_factory.mktemp("pyr11"))
+    configs.write_deck(d, *configs.pyramid_11(mg=5, n_states=8))
+    p, geo = inputs.load(d)
+    pr = pipeline.prepare(p, geo)
+    H = pipeline.assemble(pr)
+    lo, hi = eigen.index_window(pr.n_pw, p["N_VB"], p["N_CB"])
+    wr, vr = eigen.diagonalise(H, lo, hi)
+    del H
+    return d, pr, wr, vr
+
+
+def test_pyramid_11_oracle_matches_fixture(pyramid):
+    d, pr, wr, vr = pyramid
+    fx = _fixture("pyramid_11")
+    assert pr.n_h == fx["n_h"] == 10648
+    assert np.abs(wr - np.array(fx["eigenvalues_eV"])).max() < 1e-11
+
+
+@pytest.mark.parametrize("prec", [q.QD_PREC_FP64, q.QD_PREC_MIXED])
+def test_pyramid_11(pyramid, prec):
+    d, pr, wr, vr = pyramid
+    gp = q.Problem(d)
+    w, v = gp.solve(prec)
+    dE = np.abs(w - wr)
+    ang = _pair_angles(v, vr)
+    print("\npyramid_11 %s per-state |dE| (ueV):" % ("fp64" if prec == q.QD_PREC_FP64 else "mixed"),
+          np.array2string(dE * 1e6, precision=2), "\nper-pair angle (rad):", np.array2string(ang, precision=2))
+    if prec == q.QD_PREC_FP64:
+        assert dE.max() < 1e-9
+        assert ang.max() < 1e-7
+    else:
+        assert dE.max() < 1e-6
+        assert ang.max() < 1e-4
+        res, bound = last_error_bounds()
+        assert len(bound) == len(w) and bound.max() < 1e-6
+        assert np.all(dE <= np.maximum(bound, 1e-12) * 1.0001 + 1e-12)
+
+
+# --------------------------------------------------------------------------- C3
+@pytest.fixture(scope="module")
+def molecule():
+    fx = _fixture("molecule_15")
+    d = tempfile.mkdtemp(prefix="mol15_")
+    configs.write_deck(d, *configs.molecule_15(mg=7, n_states=16))
+    d32 = tempfile.mkdtemp(prefix="mol15w_")
+    configs.write_deck(d32, *configs.molecule_15(mg=7, n_states=8))
+    return fx, d, d32
+
+
+@pytest.mark.parametrize("prec", [q.QD_PREC_FP64, q.QD_PREC_MIXED])
+def test_molecule_15_window_64(molecule, prec):
+    fx, d, d32 = molecule
+    gp = q.Problem(d)
+    assert gp.n_h == fx["n_h"] == 27000 and gp.m == 64
+    w, v = gp.solve(prec)
+    wr = np.array(fx["eigenvalues_eV"])
+    dE = np.abs(w - wr)
+    mk, probes = _probes(gp.n_h, fx)
+    proj = mk.pair_projections(v, probes)
+    proj_r = np.array(fx["pair_projections"])
+    dproj = np.abs(proj - proj_r).max(axis=1) / np.abs(proj_r).max(axis=1)
+    bloch = np.abs(v.reshape(8, gp.n_pw, -1)) ** 2
+    bloch = bloch.sum(axis=1).T
+    dbloch = np.abs((bloch[0::2] + bloch[1::2]) - np.array(fx["bloch_pairs"])).max()
+    res, orth, hn = gp.residuals(w, v)
+    tag = "fp64" if prec == q.QD_PREC_FP64 else "mixed"
+    print("\nmolecule_15 %s per-state |dE| (ueV):" % tag, np.array2string(dE * 1e6, precision=2),
+          "\nper-pair probe projection rel. error:", np.array2string(dproj, precision=2),
+          "\nresidual ||Hz - Ez|| (eV):", np.array2string(res, precision=2), "orth", orth, "max|H|", hn)
+    if prec == q.QD_PREC_FP64:
+        assert dE.max() < 1e-9
+        assert dproj.max() < 1e-6
+        assert dbloch < 1e-9
+        assert res.max() < 1e-9 * max(hn, 1.0)
+        assert orth < 1e-12
+    else:
+        assert dE.max() < 1e-6
+        assert dproj.max() < 1e-3
+        assert dbloch < 1e-5
+        assert orth < 1e-10
+
+
+@pytest.mark.parametrize("prec", [q.QD_PREC_FP64, q.QD_PREC_MIXED])
+def test_molecule_15_metric_window(molecule, prec):
+    """The 32 states of the benchmark (8 e + 8 h pairs) are the middle of the
+    fixture's 64-state window."""
+    fx, d, d32 = molecule
+    gp = q.Problem(d32)
+    assert gp.m == 32
+    w, v = gp.solve(prec)
+    wr = np.array(fx["eigenvalues_eV"])[16:48]
+    dE = np.abs(w - wr)
+    print("\nmolecule_15 (32 states) per-state |dE| (ueV):", np.array2string(dE * 1e6, precision=2))
+    assert dE.max() < (1e-9 if prec == q.QD_PREC_FP64 else 1e-6)

@@ -1,6 +1,7 @@
 """Hellmann-Feynman gradients from the adjoint contraction (GPU).
 
-The truncated-pyramid deck (qudos_b200.configs.pyramid_11) at 7^3 plane waves.
+The truncated-pyramid deck (qudos_b200.configs.pyramid_11) at 7^3 plane waves
+and at its own size, 11^3 (N_H = 10648, the gradient workload).
 Parameters: dot height, base half-width, composition x (the In fraction is
 1 - x), the [001] field, and relative scales of the binary-table Ep and
 gamma_1.
@@ -25,7 +26,6 @@ from qudos_b200 import lib as L
 
 pytestmark = pytest.mark.gpu
 
-MG = 3
 BASE = dict(height=5.0, half_base=9.0, x=0.4, fz=10.0)
 PARAMS = [("height", (L.QD_GRAD_LENGTH, 1, 4)), ("half_base", (L.QD_GRAD_BASE, 1, 0)),
           ("x", (L.QD_GRAD_COMPOSITION, 1, 0)), ("fz", (L.QD_GRAD_FIELD, 0, 2)),
@@ -37,10 +37,10 @@ def need_gpu():
     assert q.device_count() > 0, "no CUDA device visible"
 
 
-def _deck(tmp, name, **kw):
+def _deck(tmp, name, mg, **kw):
     args = dict(BASE)
     args.update(kw)
-    return configs.write_deck(os.path.join(str(tmp), name), *configs.pyramid_11(mg=MG, n_states=2, cme=0, **args))
+    return configs.write_deck(os.path.join(str(tmp), name), *configs.pyramid_11(mg=mg, n_states=2, cme=0, **args))
 
 
 def _scale(name, value):
@@ -57,17 +57,18 @@ def _pairs(x):
     return 0.5 * (x[..., 0::2] + x[..., 1::2])
 
 
-@pytest.fixture(scope="module")
-def base_solution(tmp_path_factory):
-    d = _deck(tmp_path_factory.mktemp("grad"), "base")
+@pytest.fixture(scope="module", params=[3, 5], ids=["7cubed", "11cubed"])
+def base_solution(tmp_path_factory, request):
+    mg = request.param
+    d = _deck(tmp_path_factory.mktemp("grad"), "base", mg)
     pr, w, v = _solve(d)
     g = pr.gradients(v, [p for _, p in PARAMS])
-    return d, pr, w, v, g
+    return d, pr, w, v, g, mg
 
 
 @pytest.mark.parametrize("k", range(len(PARAMS)))
 def test_gradients_match_finite_differences(tmp_path, base_solution, k):
-    d, pr, w, v, g = base_solution
+    d, pr, w, v, g, mg = base_solution
     name, _ = PARAMS[k]
     rel = 1e-5
     if name in ("Ep", "gamma1"):
@@ -82,8 +83,8 @@ def test_gradients_match_finite_differences(tmp_path, base_solution, k):
             _scale(key, 1.0)
     else:
         h = rel * max(abs(BASE[name]), 1.0)
-        wp = _solve(_deck(tmp_path, "p", **{name: BASE[name] + h}))[1]
-        wm = _solve(_deck(tmp_path, "m", **{name: BASE[name] - h}))[1]
+        wp = _solve(_deck(tmp_path, "p", mg, **{name: BASE[name] + h}))[1]
+        wm = _solve(_deck(tmp_path, "m", mg, **{name: BASE[name] - h}))[1]
     fd = _pairs((wp - wm) / (2 * h))
     ad = _pairs(g[k])
     scale = np.abs(fd).max()
@@ -92,15 +93,17 @@ def test_gradients_match_finite_differences(tmp_path, base_solution, k):
 
 
 def test_gradients_match_oracle_materialised_dH(tmp_path, base_solution):
-    d, pr, w, v, g = base_solution
+    d, pr, w, v, g, mg = base_solution
     for k, name in ((0, "height"), (3, "fz"), (2, "x")):
         h = 1e-4 * max(abs(BASE[name]), 1.0)
         H = []
         for sgn in (1, -1):
-            dd = _deck(tmp_path, "o%d%s" % (sgn, name), **{name: BASE[name] + sgn * h})
+            dd = _deck(tmp_path, "o%d%s" % (sgn, name), mg, **{name: BASE[name] + sgn * h})
             p, geo = inputs.load(dd)
             H.append(pipeline.assemble(pipeline.prepare(p, geo)))
         dH = (H[0] - H[1]) / (2 * h)
-        dH = np.tril(dH) + np.tril(dH, -1).conj().T  # the oracle assembles the lower triangle
-        ref = np.real(np.einsum("is,ij,js->s", v.conj(), dH, v))
+        # the oracle assembles the lower triangle: <v|dH|v> = 2 Re(v^H L v) - v^H diag(L) v
+        ref = 2.0 * np.real(np.einsum("is,is->s", v.conj(), dH @ v)) - np.real(
+            np.einsum("is,i,is->s", v.conj(), np.diag(dH), v))
+        del H, dH
         assert np.abs(g[k] - ref).max() <= 1e-7 * np.abs(ref).max(), (name, g[k], ref)

@@ -20,7 +20,8 @@ def test_library_exports_every_declared_symbol():
     hdr = open(os.path.join(ROOT, "include", "qudos_b200.h")).read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
     names = set(re.findall(r"\b(qd_[a-z0-9_]+)\s*\(", hdr))
-    names |= {"hamiltonian_8_band", "diagonalise_hamiltonian", "eigenstates", "coulomb_matrix_elements"}
+    names |= {"hamiltonian_8_band", "diagonalise_hamiltonian", "eigenstates", "coulomb_matrix_elements",
+              "eigen_gradients_8_band", "eigenstates_batched"}
     missing = [n for n in sorted(names) if not hasattr(L.lib, n)]
     assert not missing, missing
     for g in ("N_H", "na_rows", "characteristic_function_G", "strain_G", "convolutions_char_strain",
@@ -101,3 +102,17 @@ def test_malformed_line_and_override(tmp_path):
     d = _write(tmp_path, p, c)
     with pytest.raises(q.QDError, match="override"):
         q.Problem(d, ["M_Gx=3"])
+
+
+def test_reference_arm_loads_no_native_code():
+    """bench.py --impl reference runs the oracle only: the deck writer and the
+    oracle import without loading libqdgpu.so."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import bench; bench.oracle_solve; "
+            "from qudos_b200 import configs; import oracle.pipeline; "
+            "maps = open('/proc/self/maps').read(); "
+            "print(int('qudos_b200.lib' in sys.modules), int('libqdgpu' in maps))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.split() == ["0", "0"]
