@@ -313,6 +313,11 @@ int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, int m, const
 int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void *V, const void *W, int64_t ldv, int64_t voff,
                 int K, QdTcWork *w, void *stream);
 
+/* Issuer layout of the X-product kernel: 2 (default) two MMA-issuing warps
+ * with 128 x 64 MMAs, 1 one issuer with 128 x 128 MMAs over [B_hi; B_lo].
+ * Both compute the same product; QD_XPROD_ISSUERS sets the default. */
+int qd_tc_set_xprod_issuers(int issuers);
+
 /* Per-kernel device time of the tensor-core building blocks since the last
  * call (CUDA events around every launch, on the launching stream): which 0
  * is the X product (work = bytes of the trailing matrix read, 8 m^2 per
@@ -341,6 +346,25 @@ int qd_zgemm_small_dev(int64_t n, const void *Z, int64_t ldz, int k, const void 
                        int64_t ldy, double beta, void *stream);
 int qd_residual_norms_dev(int64_t n, const void *R, int64_t ldr, const void *Z, int64_t ldz, const double *w_dev,
                           int m, double *res_dev, void *stream);
+
+/* Tall-and-skinny products of the panel steps (device pointers, column-major;
+ * fp32 != 0 selects complex64, else complex128):
+ *   qd_tsmm_nn  C[m x nc] = beta C + sum_t alpha[t] A[t] op(B[t]), nterms 1 or
+ *               2, nc <= 32; op(B) = B (K x nc, ldb) when btrans[t] == 0, else
+ *               B^H of an nc x K block;
+ *   qd_tsmm_cn  C[k1 x nc] = A^H B reduced over m rows, k1 <= 256, nc <= 32;
+ *               scratch holds qd_tsmm_cn_scratch_bytes(m, k1, nc, 8 or 16)
+ *               bytes of partial sums, which are added in FP64 in a fixed
+ *               order;
+ *   qd_small_cn C[n1 x n2] = alpha A^H B for small k x n1, k x n2 inputs. */
+int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const *A, const int64_t *lda, const void *const *B,
+               const int64_t *ldb, const int *K, const int *btrans, const double *alpha, void *C, int64_t ldc,
+               double beta, void *stream);
+int qd_tsmm_cn(int fp32, int m, const void *A, int64_t lda, int k1, const void *B, int64_t ldb, int nc, void *C,
+               int64_t ldc, void *scratch, void *stream);
+int qd_small_cn(int fp32, int k, int n1, int n2, const void *A, int lda, const void *B, int ldb, double alpha,
+                void *C, int ldc, void *stream);
+size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes);
 
 /* Residual check of host eigenpairs (m values, N_H x m vectors) of a loaded
  * problem against its H, assembled on the device in FP64:

@@ -113,30 +113,142 @@ __device__ zc band_element(const Ctx &c, int rb, int cb, const int r[3], const i
     return c_fac[rb][cb] * v;
 }
 
-template <int OUT>  // OUT: 1 complex128, 2 complex64, 3 both
-__global__ void __launch_bounds__(128) assemble_kernel(Ctx c, int64_t npw, int64_t nh, double2 *__restrict__ H64,
-                                                       float2 *__restrict__ H32, int64_t ld, int full, int cols_per) {
-    int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t col0 = (int64_t)blockIdx.y * cols_per;
-    int64_t row_first = blockIdx.x * (int64_t)blockDim.x;
-    if (!full && row_first + blockDim.x - 1 < col0) return;  // tile entirely above the diagonal
-    if (row >= nh) return;
-    int rb = (int)(row / npw);
-    int i = (int)(row - rb * npw);
-    int r[3] = {i / (c.N[1] * c.N[2]), (i / c.N[2]) % c.N[1], i % c.N[2]};
-    int64_t col_end = col0 + cols_per < nh ? col0 + cols_per : nh;
-    for (int64_t col = col0; col < col_end; col++) {
-        if (!full && row < col) break;
-        int cb = (int)(col / npw);
-        int j = (int)(col - cb * npw);
-        int q[3] = {j / (c.N[1] * c.N[2]), (j / c.N[2]) % c.N[1], j % c.N[2]};
-        zc v;
-        if (row >= col) v = band_element(c, rb, cb, r, q);
-        else v = conj(band_element(c, cb, rb, q, r));
-        int64_t o = row + ld * col;
-        if (OUT & 1) __stcs(&H64[o], v.d2());
-        if (OUT & 2) __stcs(&H32[o], make_float2((float)v.re, (float)v.im));
+// Band-block map of hamiltonian_8_band.c:78-492 as compile-time functions of
+// (row band, column band), row band >= column band, 0-based; the same table
+// as upload_block_map below, in a form the unrolled block loop folds away.
+__host__ __device__ constexpr int bfunc(int rb, int cb) {
+    switch (rb * 8 + cb) {
+        case 0: return F_ECB;  case 8: return F_TM;  case 16: return F_U;   case 24: return F_U;
+        case 48: return F_TP;  case 56: return F_TP;
+        case 9: return F_EHH;  case 17: return F_SC; case 25: return F_SC;  case 49: return F_RC; case 57: return F_RC;
+        case 18: return F_ELH; case 26: return F_Q;  case 34: return F_TP;  case 42: return F_RC; case 58: return F_SC;
+        case 27: return F_ESO; case 35: return F_TP; case 43: return F_RC;  case 51: return F_SC;
+        case 36: return F_ECB; case 44: return F_TP; case 52: return F_U;   case 60: return F_U;
+        case 45: return F_EHH; case 53: return F_S;  case 61: return F_S;
+        case 54: return F_ELH; case 62: return F_Q;
+        case 63: return F_ESO;
+        default: return F_ZERO;
     }
+}
+__host__ __device__ constexpr double bfac(int rb, int cb) {
+    switch (rb * 8 + cb) {
+        case 8: return -1.7320508075688772;   case 16: return 1.4142135623730951; case 24: return -1.0;
+        case 48: return -1.0;                 case 56: return -1.4142135623730951;
+        case 17: return 1.4142135623730951;  case 25: return -1.0; case 49: return -1.0; case 57: return -1.4142135623730951;
+        case 58: return 1.7320508075688772;
+        case 35: return 1.4142135623730951;  case 43: return 1.4142135623730951; case 51: return -1.7320508075688772;
+        case 44: return -1.7320508075688772; case 52: return 1.4142135623730951; case 60: return -1.0;
+        case 53: return 1.4142135623730951;  case 61: return -1.0;
+        default: return 1.0;
+    }
+}
+
+// All twelve band functions of one (row plane wave, column plane wave) pair:
+// v[F_*], from the fused coefficients at difference index t (each field
+// loaded once) and the two plane waves' G (g1: row, g2: column).
+__device__ __forceinline__ void band_values(const Ctx &c, int64_t t, const double g1[3], const double g2[3],
+                                            zc (&v)[13]) {
+    const double Kx = c.K[0], Ky = c.K[1], Kz = c.K[2];
+    const double g1x = g1[0], g1y = g1[1], g1z = g1[2], g2x = g2[0], g2y = g2[1], g2z = g2[2];
+    const double kinx = g1x * g2x + Kx * (g1x + g2x), kiny = g1y * g2y + Ky * (g1y + g2y),
+                 kinz = g1z * g2z + Kz * (g1z + g2z);
+    const double kxy = kinx + kiny + Kx * Kx + Ky * Ky, kzz = kinz + Kz * Kz, kall = kxy + kzz;
+    const double H2 = 0.5 * QD_HBSQM;
+    const zc f10 = ld(c, 10, t), f11 = ld(c, 11, t), P = ld(c, 12, t);
+    v[F_ZERO] = zc(0.0);
+    v[F_ECB] = ld(c, 0, t) + H2 * ld(c, 1, t) * kall + ld(c, 13, t);
+    v[F_EHH] = ld(c, 2, t) - H2 * ld(c, 3, t) * kxy - H2 * ld(c, 4, t) * kzz + ld(c, 14, t);
+    v[F_ELH] = ld(c, 5, t) - H2 * ld(c, 6, t) * kxy - H2 * ld(c, 7, t) * kzz + ld(c, 15, t);
+    v[F_ESO] = ld(c, 8, t) - H2 * ld(c, 9, t) * kall + ld(c, 16, t);
+    v[F_Q] = (-sqrt(0.5) * QD_HBSQM) * f10 * kxy + (sqrt(2.0) * QD_HBSQM) * f10 * kzz + ld(c, 17, t);
+    {
+        const double a = 0.5 * sqrt(3.0) * QD_HBSQM;
+        const zc kin = a * f10 * (kinx - kiny + Kx * Kx - Ky * Ky);
+        const zc off = a * f11 * ((g1x + Kx) * (g2y + Ky) + (g1y + Ky) * (g2x + Kx));
+        const zc r18 = ld(c, 18, t), rd = ld(c, 19, t);
+        v[F_R] = kin - I_times(off) + r18 + I_times(rd);   // sg = -1
+        v[F_RC] = kin + I_times(off) + r18 - I_times(rd);  // sg = +1
+    }
+    {
+        const double a = 0.5 * sqrt(1.5) * QD_HBSQM;
+        const zc re = a * f11 * ((g1x + Kx) * (g2z + Kz) + (g1z + Kz) * (g2x + Kx));
+        const zc im = a * f11 * ((g1y + Ky) * (g2z + Kz) + (g1z + Kz) * (g2y + Ky));
+        const zc sxz = ld(c, 20, t), syz = ld(c, 21, t);
+        v[F_S] = re - I_times(im) - sqrt(0.5) * (sxz - I_times(syz));
+        v[F_SC] = re + I_times(im) - sqrt(0.5) * (sxz + I_times(syz));
+    }
+    {
+        const double kx = g1x + g2x + 2 * Kx, ky = g1y + g2y + 2 * Ky, kz = g1z + g2z + 2 * Kz;
+        const zc Txx = ld(c, 22, t), Txy = ld(c, 23, t), Tyy = ld(c, 24, t), Txz = ld(c, 25, t), Tyz = ld(c, 26, t);
+        const double c6 = -0.5 / sqrt(6.0), i26 = 1.0 / (2.0 * sqrt(6.0));
+        const zc base = Txx * kx + Txy * ky + Txz * kz;  // part of the strain sum without the +-i factor
+        const zc sI = Txy * kx + Tyy * ky + Tyz * kz;    // part multiplied by +-i
+        const zc p0 = (P * kx) * i26, p1 = I_times(P * ky) * i26;
+        v[F_TP] = p0 + p1 + c6 * (base + I_times(sI));
+        v[F_TM] = p0 - p1 + c6 * (base - I_times(sI));
+        const double c3 = -0.5 / sqrt(3.0);
+        v[F_U] = (P * kz) / (2.0 * sqrt(3.0)) + c3 * (Txz * kx + Tyz * ky + ld(c, 27, t) * kz);
+    }
+}
+
+__device__ __forceinline__ int64_t diff_index(const Ctx &c, const int r[3], const int q[3]) {
+    return ((int64_t)(r[0] - q[0] + c.NT[0] / 2) * c.NT[1] + (r[1] - q[1] + c.NT[1] / 2)) * c.NT[2] +
+           (r[2] - q[2] + c.NT[2] / 2);
+}
+
+// One thread per (row plane wave r, column plane wave q): the twelve band
+// functions are evaluated once for the pair (twice when an output needs the
+// upper triangle: the upper elements are conjugates of the lower ones of the
+// pair (q, r)), and the 8 x 8 band block is written out.  Threads of a warp
+// hold 32 consecutive r for one q, so every store of a band block is 32
+// consecutive elements of one column.  Stores: complex128 into H64 (lower
+// triangle, or full with F64), complex64 into H32 (lower or full with F32).
+template <bool W64, bool F64, bool W32, bool F32>
+__global__ void __launch_bounds__(256) assemble_pw_kernel(Ctx c, int npw, double2 *__restrict__ H64, int64_t ld64,
+                                                          float2 *__restrict__ H32, int64_t ld32) {
+    const int r = blockIdx.x * 32 + threadIdx.x;
+    const int q = blockIdx.y * 8 + threadIdx.y;
+    if (r >= npw || q >= npw) return;
+    const int nyz = c.N[1] * c.N[2];
+    const int ir[3] = {r / nyz, (r / c.N[2]) % c.N[1], r % c.N[2]};
+    const int iq[3] = {q / nyz, (q / c.N[2]) % c.N[1], q % c.N[2]};
+    double g1[3], g2[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        g1[a] = __ldg(&c.G[a][c.off[a] + ir[a]]);
+        g2[a] = __ldg(&c.G[a][c.off[a] + iq[a]]);
+    }
+    zc v[13], u[13];
+    band_values(c, diff_index(c, ir, iq), g1, g2, v);
+    constexpr bool need_upper = (W64 && F64) || (W32 && F32);
+    if (need_upper) band_values(c, diff_index(c, iq, ir), g2, g1, u);
+#pragma unroll
+    for (int cb = 0; cb < 8; cb++) {
+#pragma unroll
+        for (int rb = 0; rb < 8; rb++) {
+            const int64_t row = (int64_t)rb * npw + r, col = (int64_t)cb * npw + q;
+            const bool lower = rb > cb || (rb == cb && r >= q);
+            zc val;
+            if (lower) {
+                val = bfac(rb, cb) * v[bfunc(rb, cb)];
+            } else {
+                if (!need_upper) continue;
+                val = conj(bfac(cb, rb) * u[bfunc(cb, rb)]);
+            }
+            if (W64 && (lower || F64)) __stcs(&H64[row + ld64 * col], val.d2());
+            if (W32 && (lower || F32)) __stcs(&H32[row + ld32 * col], make_float2((float)val.re, (float)val.im));
+        }
+    }
+}
+
+template <bool W64, bool F64, bool W32, bool F32>
+int launch_pw(const Ctx &c, int npw, double2 *H64, int64_t ld64, float2 *H32, int64_t ld32, cudaStream_t st) {
+    dim3 grid((unsigned)((npw + 31) / 32), (unsigned)((npw + 7) / 8)), block(32, 8);
+    qd_count_launch(1);
+    assemble_pw_kernel<W64, F64, W32, F32><<<grid, block, 0, st>>>(c, npw, H64, ld64, H32, ld32);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
+    return QD_OK;
 }
 
 int upload_block_map() {
@@ -182,20 +294,15 @@ extern "C" int qd_assemble_launch(const void *d_coef, const double *d_Gx, const 
     c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
     int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
     if (ld < nh) return qd_set_error(QD_ERR_ARG, "leading dimension %lld < N_H %lld", (long long)ld, (long long)nh);
-    const int cols_per = 16;
-    dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
     cudaStream_t st = (cudaStream_t)stream;
-    int full = mode == 1;
-    qd_count_launch(1);
+    const int full = mode == 1;
     if (prec == QD_PREC_FP64)
-        assemble_kernel<1><<<grid, 128, 0, st>>>(c, npw, nh, (double2 *)H, nullptr, ld, full, cols_per);
-    else if (prec == QD_PREC_MIXED)
-        assemble_kernel<2><<<grid, 128, 0, st>>>(c, npw, nh, nullptr, (float2 *)H, ld, full, cols_per);
-    else
-        return qd_set_error(QD_ERR_ARG, "unknown precision %d", prec);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
-    return QD_OK;
+        return full ? launch_pw<true, true, false, false>(c, (int)npw, (double2 *)H, ld, nullptr, 0, st)
+                    : launch_pw<true, false, false, false>(c, (int)npw, (double2 *)H, ld, nullptr, 0, st);
+    if (prec == QD_PREC_MIXED)
+        return full ? launch_pw<false, false, true, true>(c, (int)npw, nullptr, 0, (float2 *)H, ld, st)
+                    : launch_pw<false, false, true, false>(c, (int)npw, nullptr, 0, (float2 *)H, ld, st);
+    return qd_set_error(QD_ERR_ARG, "unknown precision %d", prec);
 }
 
 // Both copies in one pass: complex128 into H64 and complex64 into H32 (same ld).
@@ -214,14 +321,12 @@ extern "C" int qd_assemble_dual_launch(const void *d_coef, const double *d_Gx, c
     }
     c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
     int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
-    const int cols_per = 16;
-    dim3 grid((unsigned)((nh + 127) / 128), (unsigned)((nh + cols_per - 1) / cols_per));
-    qd_count_launch(1);
-    assemble_kernel<3><<<grid, 128, 0, (cudaStream_t)stream>>>(c, npw, nh, (double2 *)H64, (float2 *)H32, ld,
-                                                                mode == 1, cols_per);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
-    return QD_OK;
+    (void)nh;
+    // complex128 lower triangle (the reference's layout) and the full Hermitian complex64 copy
+    return mode == 1 ? launch_pw<true, true, true, true>(c, (int)npw, (double2 *)H64, ld, (float2 *)H32, ld,
+                                                         (cudaStream_t)stream)
+                     : launch_pw<true, false, true, true>(c, (int)npw, (double2 *)H64, ld, (float2 *)H32, ld,
+                                                          (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -76,14 +76,46 @@ extern "C" void qd_set_timing(int i, double ms) {
 // ---------------------------------------------------------------------------
 // small kernels
 // ---------------------------------------------------------------------------
-// full Hermitian complex64 copy of a complex128 lower triangle
-__global__ void lower64_to_full32_kernel(const double2 *H, int64_t ld, int64_t n, float2 *H32, int64_t ld32) {
-    int64_t col = blockIdx.y;
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
-        double2 v = row >= col ? H[row + col * ld] : H[col + row * ld];
-        if (row < col) v.y = -v.y;
-        if (row == col) v.y = 0.0;
-        H32[row + col * ld32] = make_float2((float)v.x, (float)v.y);
+// Full Hermitian complex64 copy of a complex128 lower triangle, by 32 x 32
+// tiles of the lower triangle: tile (I, J), I >= J, is read once (coalesced
+// down its columns), written to (I, J) and, conjugate-transposed through
+// shared memory, to (J, I), so that both stores are coalesced too.  Only the
+// lower triangle is read; the diagonal comes out real.
+__global__ void __launch_bounds__(256) lower64_to_full32_kernel(const double2 *__restrict__ H, int64_t ld, int n,
+                                                                float2 *__restrict__ H32, int64_t ld32) {
+    __shared__ float2 tile[32][33];
+    const int T = (n + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32 threads
+    for (int64_t item = blockIdx.x; item < (int64_t)T * (T + 1) / 2; item += gridDim.x) {
+        // item -> (I, J), I >= J: I (I + 1) / 2 <= item < (I + 1) (I + 2) / 2
+        int I = (int)((sqrt(8.0 * (double)item + 1.0) - 1.0) * 0.5);
+        while ((int64_t)I * (I + 1) / 2 > item) I--;
+        while ((int64_t)(I + 1) * (I + 2) / 2 <= item) I++;
+        const int J = (int)(item - (int64_t)I * (I + 1) / 2);
+        const int r0 = 32 * I, c0 = 32 * J;
+        // tile[a][b] holds element (r0 + b, c0 + a)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int row = r0 + tx, col = c0 + ty + 8 * k;
+            float2 v = make_float2(0.f, 0.f);
+            if (row < n && col < n && row >= col) {
+                const double2 h = H[row + (int64_t)col * ld];
+                v = make_float2((float)h.x, row == col ? 0.f : (float)h.y);
+                H32[row + (int64_t)col * ld32] = v;
+            }
+            tile[ty + 8 * k][tx] = v;
+        }
+        __syncthreads();
+        // strictly upper element (c0 + tx, r0 + ty + 8 k) = conj(element (r0 + ty + 8 k, c0 + tx))
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int row = c0 + tx, col = r0 + ty + 8 * k;
+            if (row < n && col < n && row < col) {
+                const float2 v = tile[tx][ty + 8 * k];
+                H32[row + (int64_t)col * ld32] = make_float2(v.x, -v.y);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -401,8 +433,7 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     if (mixed) {
         CUDA_OK((cudaError_t)qd_pool_alloc((void **)&H32, sizeof(float2) * n * n, st));
         qd_count_launch(1);
-        lower64_to_full32_kernel<<<dim3((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)n), 256, 0, st>>>(
-            (const double2 *)H, ld, n, H32, n);
+        lower64_to_full32_kernel<<<148 * 8, 256, 0, st>>>((const double2 *)H, ld, (int)n, H32, n);
         CUDA_OK(cudaGetLastError());
         A = H32;
         lda = n;

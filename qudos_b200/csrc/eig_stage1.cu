@@ -326,6 +326,48 @@ static int n_panels(int64_t n, int b) {
 
 extern "C" cublasHandle_t qd_cublas(void);
 extern "C" int qd_mixed_gemm_mode(void);
+extern "C" int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const *A, const int64_t *lda,
+                          const void *const *B, const int64_t *ldb, const int *K, const int *btrans,
+                          const double *alpha, void *C, int64_t ldc, double beta, void *stream);
+extern "C" int qd_tsmm_cn(int fp32, int m, const void *A, int64_t lda, int k1, const void *B, int64_t ldb, int nc,
+                          void *C, int64_t ldc, void *scratch, void *stream);
+extern "C" int qd_small_cn(int fp32, int k, int n1, int n2, const void *A, int lda, const void *B, int ldb,
+                           double alpha, void *C, int ldc, void *stream);
+extern "C" size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes);
+
+// One- or two-term tall product C[m x nc] = beta C + sum alpha_t A_t op(B_t),
+// 32 output columns per launch.
+template <typename T>
+static int nn(cudaStream_t st, int m, int nc, const T *A0, int64_t lda0, const T *B0, int64_t ldb0, int K0, int bt0,
+              double al0, T *C, int64_t ldc, double beta, const T *A1 = nullptr, int64_t lda1 = 0,
+              const T *B1 = nullptr, int64_t ldb1 = 0, int K1 = 0, int bt1 = 0, double al1 = 0.0) {
+    const void *A[2] = {A0, A1}, *B[2] = {B0, B1};
+    int64_t la[2] = {lda0, lda1}, lb[2] = {ldb0, ldb1};
+    int K[2] = {K0, K1}, bt[2] = {bt0, bt1};
+    double al[2] = {al0, al1};
+    const int fp32 = sizeof(T) == 8;
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+        const int w = nc - c0 < 32 ? nc - c0 : 32;
+        const void *Bc[2];
+        for (int t = 0; t < 2; t++)
+            Bc[t] = B[t] ? (const void *)((const T *)B[t] + (bt[t] ? c0 : c0 * lb[t])) : nullptr;
+        int rc = qd_tsmm_nn(fp32, m, w, A1 ? 2 : 1, A, la, Bc, lb, K, bt, al, C + c0 * ldc, ldc, beta, st);
+        if (rc) return rc;
+    }
+    return QD_OK;
+}
+// C[k1 x nc] = A[m x k1]^H B[m x nc] (k1 <= 256), 32 output columns per launch.
+template <typename T>
+static int cn(cudaStream_t st, int m, const T *A, int64_t lda, int k1, const T *B, int64_t ldb, int nc, T *C,
+              int64_t ldc, void *part) {
+    const int fp32 = sizeof(T) == 8;
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+        const int w = nc - c0 < 32 ? nc - c0 : 32;
+        int rc = qd_tsmm_cn(fp32, m, A, lda, k1, B + c0 * ldb, ldb, w, C + c0 * ldc, ldc, part, st);
+        if (rc) return rc;
+    }
+    return QD_OK;
+}
 extern "C" int qd_tc_work_alloc_on(int64_t n, int kmax, QdTcWork **out, cudaStream_t st);
 extern "C" void qd_tc_work_free_on(QdTcWork *w, cudaStream_t st);
 
@@ -463,7 +505,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
     const bool full = sizeof(R) == 4;
     cublasHandle_t h = qd_cublas();
     BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
-    const T one = cval<T>(1, 0), zero = cval<T>(0, 0), mone = cval<T>(-1, 0), mhalf = cval<T>(-0.5, 0);
+    const T one = cval<T>(1, 0), zero = cval<T>(0, 0), mone = cval<T>(-1, 0);
     const cublasOperation_t N_ = CUBLAS_OP_N, C_ = CUBLAS_OP_C;
     T *Vacc = (T *)w.Vacc, *Wacc = (T *)w.Wacc;
     const int64_t ldv = w.ldv;
@@ -478,12 +520,9 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         T *Pcol = A + k + k * lda;  // rows k.., columns k..k+nb-1
         // 1. bring the panel's b columns up to date with the pending (V, W) terms
         prof_mark(0, st);
-        if (K > 0) {
-            BLAS_OK(Blas<T>::gemm(h, N_, C_, (int)(n - k), b, K, &mone, Vacc + off, ldv, Wacc + off, ldv, &one, Pcol,
-                                  lda));
-            BLAS_OK(Blas<T>::gemm(h, N_, C_, (int)(n - k), b, K, &mone, Wacc + off, ldv, Vacc + off, ldv, &one, Pcol,
-                                  lda));
-        }
+        if (K > 0)  // P -= V Wb^H + W Vb^H
+            RC(nn<T>(st, (int)(n - k), b, Vacc + off, ldv, Wacc + off, ldv, K, 1, -1.0, Pcol, lda, 1.0, Wacc + off,
+                     ldv, Vacc + off, ldv, K, 1, -1.0));
         // 2. panel QR -> V (explicit, in place), tau, R; nb = min(b, m) reflectors over all b columns
         T *P = A + (k + b) + k * lda;
         prof_mark(1, st);
@@ -491,7 +530,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         RC(launch_panel<T>(P, lda, m, b, nb, Rp, (T *)w.tau, w, st));
         // 3. T from the Gram matrix
         prof_mark(2, st);
-        BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, m, &one, P, lda, P, lda, &zero, (T *)w.gram, b));
+        RC(cn<T>(st, m, P, lda, nb, P, lda, nb, (T *)w.gram, b, w.part));
         qd_count_launch(1);
         {
             static int ft_configured[2] = {0, 0};
@@ -509,7 +548,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         T *VT = (T *)w.VT;
         T *X = Wacc + (off + b) + (int64_t)K * ldv;
         T *A22 = A + (k + b) + (k + b) * lda;
-        BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, nb, &one, P, lda, Tp, b, &zero, VT, m));
+        RC(nn<T>(st, m, nb, P, lda, Tp, b, nb, 0, 1.0, VT, m, 0.0));
         prof_mark(3, st);
         if (full && w.tc) {
             RC(qd_tc_xprod(A, lda, n, k + b, m, VT, m, nb, X, ldv, w.tc, st));
@@ -523,16 +562,16 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         prof_mark(4, st);
         if (K > 0) {
             T *S1 = (T *)w.S1, *S2 = (T *)w.S2;
-            BLAS_OK(Blas<T>::gemm(h, C_, N_, K, nb, m, &one, Wacc + off + b, ldv, VT, m, &zero, S1, w.agg));
-            BLAS_OK(Blas<T>::gemm(h, C_, N_, K, nb, m, &one, Vacc + off + b, ldv, VT, m, &zero, S2, w.agg));
-            BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, K, &mone, Vacc + off + b, ldv, S1, w.agg, &one, X, ldv));
-            BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, K, &mone, Wacc + off + b, ldv, S2, w.agg, &one, X, ldv));
+            RC(cn<T>(st, m, Wacc + off + b, ldv, K, VT, m, nb, S1, w.agg, w.part));
+            RC(cn<T>(st, m, Vacc + off + b, ldv, K, VT, m, nb, S2, w.agg, w.part));
+            RC(nn<T>(st, m, nb, Vacc + off + b, ldv, S1, w.agg, K, 0, -1.0, X, ldv, 1.0, Wacc + off + b, ldv, S2,
+                     w.agg, K, 0, -1.0));
         }
         // 6. W = X - 1/2 V (T^H V^H X)
         prof_mark(5, st);
-        BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, m, &one, P, lda, X, ldv, &zero, (T *)w.M, b));
-        BLAS_OK(Blas<T>::gemm(h, C_, N_, nb, nb, nb, &one, Tp, b, (T *)w.M, b, &zero, (T *)w.Y, b));
-        BLAS_OK(Blas<T>::gemm(h, N_, N_, m, nb, nb, &mhalf, P, lda, (T *)w.Y, b, &one, X, ldv));
+        RC(cn<T>(st, m, P, lda, nb, X, ldv, nb, (T *)w.M, b, w.part));
+        RC(qd_small_cn(sizeof(T) == 8, nb, nb, nb, Tp, b, w.M, b, 1.0, w.Y, b, st));
+        RC(nn<T>(st, m, nb, P, lda, (T *)w.Y, b, nb, 0, -0.5, X, ldv, 1.0));
         // 7. append V (zero above its first row) to Vacc; W already sits in Wacc
         prof_mark(6, st);
         CUDA_OK(cudaMemset2DAsync(Vacc + (int64_t)K * ldv, sizeof(T) * ldv, 0, sizeof(T) * (off + b), nb, st));
@@ -579,10 +618,10 @@ extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, 
     w->ldv = n;
     size_t eb = (size_t)elem_bytes;
     void **bufs[] = {&w->VT, &w->X, &w->M, &w->Y, &w->Tall, &w->Rall, &w->Vacc, &w->Wacc, &w->S1, &w->S2, &w->gram,
-                     &w->tau};
+                     &w->tau, &w->part};
     size_t sizes[] = {eb * n * b, eb * 16, eb * b * b, eb * b * b, eb * (size_t)(w->npanels + 1) * b * b,
                       eb * (size_t)(w->npanels + 1) * b * b, eb * n * agg, eb * n * agg, eb * agg * b,
-                      eb * agg * b, eb * b * b, eb * b};
+                      eb * agg * b, eb * b * b, eb * b, qd_tsmm_cn_scratch_bytes((int)n, agg, 32, (int)eb)};
     for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); i++)
         if (qd_pool_alloc(bufs[i], sizes[i], st) != 0) return qd_set_error(QD_ERR_NOMEM, "stage-1 workspace");
     int dev, nsm;
@@ -604,7 +643,7 @@ extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, 
 
 extern "C" void qd_stage1_free(Stage1Work *w, cudaStream_t st) {
     void *p[] = {w->VT, w->X, w->M, w->Y, w->Tall, w->Rall, w->Vacc, w->Wacc, w->S1, w->S2, w->gram, w->tau,
-                 w->red, w->rowbuf, w->bar, w->err};
+                 w->part, w->red, w->rowbuf, w->bar, w->err};
     for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) qd_pool_free(p[i], st);
     if (w->tc) qd_tc_work_free_on(w->tc, st);
     w->tc = nullptr;
@@ -672,9 +711,6 @@ extern "C" int qd_extract_band(const void *A, int64_t n, int64_t lda, int b, int
 template <typename T>
 static int backtransform(const T *A, int64_t n, int64_t lda, int b, const Stage1Work *w, T *Z, int64_t ldz, int mz,
                          cudaStream_t st) {
-    cublasHandle_t h = qd_cublas();
-    BLAS_OK(cublasSetStream(h, st ? st : cudaStreamPerThread));
-    const T one = cval<T>(1, 0), zero = cval<T>(0, 0), mone = cval<T>(-1, 0);
     for (int p = w->npanels - 1; p >= 0; p--) {
         int64_t k = (int64_t)p * b;
         int m = (int)(n - k - b), nb = b < m ? b : m;
@@ -682,9 +718,9 @@ static int backtransform(const T *A, int64_t n, int64_t lda, int b, const Stage1
         const T *Tm = (const T *)w->Tall + (int64_t)p * b * b;
         T *Zs = Z + (k + b);
         T *M = (T *)w->VT, *Y = (T *)w->Vacc;
-        BLAS_OK(Blas<T>::gemm(h, CUBLAS_OP_C, CUBLAS_OP_N, nb, mz, m, &one, V, lda, Zs, ldz, &zero, M, nb));
-        BLAS_OK(Blas<T>::gemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nb, mz, nb, &one, Tm, b, M, nb, &zero, Y, nb));
-        BLAS_OK(Blas<T>::gemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, mz, nb, &mone, V, lda, Y, nb, &one, Zs, ldz));
+        RC(cn<T>(st, m, V, lda, nb, Zs, ldz, mz, M, nb, w->part));     // M = V^H Z
+        RC(nn<T>(st, nb, mz, Tm, b, M, nb, nb, 0, 1.0, Y, nb, 0.0));    // Y = T M
+        RC(nn<T>(st, m, mz, V, lda, Y, nb, nb, 0, -1.0, Zs, ldz, 1.0));  // Z -= V Y
     }
     return QD_OK;
 }

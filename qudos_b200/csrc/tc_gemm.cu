@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include <vector>
 
@@ -330,8 +331,12 @@ constexpr int X_L_COL0 = 2 * X_ISSUERS * X_N;
 constexpr int X_TMEM_COLS = 512;
 static_assert(X_L_COL0 + 2 * BKF * XL_STAGES <= X_TMEM_COLS, "TMEM columns");
 
-// Epilogue of the X product: every accumulation chunk is the sum of the two
-// issuers' accumulators (columns 64 (2 h + ab) of this warp's lane quarter).
+// Epilogue of the X product: every accumulation chunk is the sum of two
+// 64-column accumulators of this warp's lane quarter.  With two issuers (ISS
+// = 2) they are the issuers' accumulators, at columns 64 (2 h + ab); with one
+// issuer (ISS = 1) the two halves of its 128-column accumulator at 128 ab
+// (hi*hi + lo*hi in the first half, hi*lo in the second).
+template <int ISS>
 __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t tmem_base, int q, int &ab,
                                            uint32_t &aphase, uint64_t *tfull, uint64_t *tempty,
                                            volatile int *abort_flag) {
@@ -341,9 +346,10 @@ __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t 
         if (!mbar_wait_warp(&tfull[ab], aphase, abort_flag)) return false;
         tc_fence_after();
 #pragma unroll
-        for (int h = 0; h < X_ISSUERS; h++) {
+        for (int h = 0; h < 2; h++) {
             uint32_t v[X_N];
-            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((h * 2 + ab) * X_N);
+            const uint32_t col = ISS == 2 ? (uint32_t)((h * 2 + ab) * X_N) : (uint32_t)(ab * 2 * X_N + h * X_N);
+            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + col;
             tmem_ld32_issue(ta, v);
             tmem_ld32_issue(ta + 32, v + 32);
             tmem_ld_wait();
@@ -361,6 +367,15 @@ __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t 
     return true;
 }
 
+// ISS = 2: two MMA-issuing warps (1 and 11), each with its own double-buffered
+// 64-column accumulator, K steps 2h and 2h + 1 of every k-block, three
+// 128 x 64 x 8 MMAs per K step (hi*hi, hi*lo, lo*hi).
+// ISS = 1: warp 1 alone issues every K step as two MMAs: 128 x 128 x 8 with B
+// = [B_hi; B_lo] (the two 64-row halves of the B stage are adjacent, so one
+// descriptor spans both: hi*hi and hi*lo at once) and 128 x 64 x 8 lo*hi into
+// the first half; eight MMAs per k-block instead of twelve, each A tile read
+// from tensor memory twice instead of three times.
+template <int ISS>
 __global__ void __launch_bounds__(X_WARPS * 32, 1)
     xprod_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
@@ -387,13 +402,13 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         for (int s = 0; s < XB_STAGES; s++) mbar_init(&fullB[s], 1);
         for (int s = 0; s < XL_STAGES; s++) {
             mbar_init(&conv[s], 4);  // one arrival per converter warp
-            mbar_init(&emptyL[s], X_ISSUERS);
+            mbar_init(&emptyL[s], ISS);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&tfull[b], X_ISSUERS);
+            mbar_init(&tfull[b], ISS);
             mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
-        mbar_init(done, X_ISSUERS);
+        mbar_init(done, ISS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -453,9 +468,9 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         }
     } else if (warp == 1 || warp == 11) {
         // ---------------- MMA issuers (accumulation restarted every X_CHUNK k-blocks) ----------------
-        if (lane == 0) {
-            const int h = warp == 11;  // K steps 2h, 2h + 1 of every k-block
-            const uint32_t idesc = tf32_idesc(TILE_M, X_N);
+        if (lane == 0 && (ISS == 2 || warp == 1)) {
+            const int h = warp == 11;  // ISS = 2: K steps 2h, 2h + 1 of every k-block
+            const uint32_t idesc = tf32_idesc(TILE_M, X_N), idesc2 = tf32_idesc(TILE_M, 2 * X_N);
             const uint64_t bdesc0 = sw128_desc(smem_u32(ringB));
             int sb = 0, sl = 0, ab = 0;
             uint32_t pb = 0, pl = 0, aphase = 0;
@@ -479,18 +494,31 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d = tmem_base + (uint32_t)((h * 2 + ab) * X_N);
-                    const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF + h * 16);
-                    const uint32_t a_lo = a_hi + BKF;
-                    // +32 bytes along K in the B tile = +2 in the descriptor's address field
-                    const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES + h * 64) >> 4);
-                    const uint64_t bl = bh + (X_B_BYTES >> 4);
+                    if (ISS == 2) {
+                        const uint32_t d = tmem_base + (uint32_t)((h * 2 + ab) * X_N);
+                        const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF + h * 16);
+                        const uint32_t a_lo = a_hi + BKF;
+                        // +32 bytes along K in the B tile = +2 in the descriptor's address field
+                        const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES + h * 64) >> 4);
+                        const uint64_t bl = bh + (X_B_BYTES >> 4);
 #pragma unroll
-                    for (int kk = 0; kk < 2; kk++) {
-                        uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
-                        umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc, acc);
-                        umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
-                        umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
+                        for (int kk = 0; kk < 2; kk++) {
+                            uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
+                            umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc, acc);
+                            umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
+                            umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
+                        }
+                    } else {
+                        const uint32_t d = tmem_base + (uint32_t)(ab * 2 * X_N);
+                        const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF);
+                        const uint32_t a_lo = a_hi + BKF;
+                        const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES) >> 4);
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) {
+                            uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
+                            umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc2, acc);  // [hi*hi | hi*lo]
+                            umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);    // + lo*hi (first half)
+                        }
                     }
                     umma_commit(&emptyL[sl]);  // frees B stage sb == sl and TMEM stage sl
                     ring_next(sb, pb, XB_STAGES);
@@ -516,8 +544,8 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             int tm, sp, kb0, kb1;
             xprod_item(args, item, tm, sp, kb0, kb1);
             float acc[X_N];
-            if (!drain_pair(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, ab, aphase, tfull, tempty,
-                            abort_flag)) {
+            if (!drain_pair<ISS>(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, ab, aphase, tfull, tempty,
+                                 abort_flag)) {
                 fail(4);
                 break;
             }
@@ -932,19 +960,35 @@ void timer_mark(int which, cudaStream_t st) {
     cudaEventRecord(t.ev[t.used++], st);
 }
 
+// Issuer layout of the X product: 1 selects the single issuer with
+// 128-column MMAs, 2 the two issuers (QD_XPROD_ISSUERS in the environment, or
+// qd_tc_set_xprod_issuers).
+int g_xprod_issuers = -1;
+int xprod_issuers() {
+    if (g_xprod_issuers < 0) {
+        const char *e = getenv("QD_XPROD_ISSUERS");
+        g_xprod_issuers = (e && atoi(e) == 1) ? 1 : 2;
+    }
+    return g_xprod_issuers;
+}
+
 int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &blo, const TcArgs &args,
                  cudaStream_t st) {
     static bool configured = false;
     const int smem = X_SMEM + SMEM_EXTRA;
     if (!configured) {
-        CUDA_OK(cudaFuncSetAttribute(xprod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_OK(cudaFuncSetAttribute(xprod_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_OK(cudaFuncSetAttribute(xprod_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         configured = true;
     }
     int grid = args.n_items < sm_count() ? args.n_items : sm_count();
     if (grid < 1) return QD_OK;
     qd_count_launch(1);
     timer_mark(0, st);
-    xprod_kernel<<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
+    if (xprod_issuers() == 1)
+        xprod_kernel<1><<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
+    else
+        xprod_kernel<2><<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
     CUDA_OK(cudaGetLastError());
     timer_mark(0, st);
     g_timer[0].work += 8.0 * (double)args.rows * (double)args.rows;
@@ -972,8 +1016,13 @@ int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap
 
 }  // namespace
 
-// Work buffers of the tensor-core path (device), sized for an n x n matrix
-// and rank-2K updates with K <= kmax.
+extern "C" int qd_tc_set_xprod_issuers(int issuers) {
+    if (issuers != 1 && issuers != 2) return qd_set_error(QD_ERR_ARG, "X product issuers must be 1 or 2");
+    g_xprod_issuers = issuers;
+    return QD_OK;
+}
+
+// Limit of the pipeline waits for the current device (ns; negative: default).
 extern "C" int qd_tc_set_wait_limit(long long ns) {
     const unsigned long long v = ns < 0 ? WAIT_NS_DEFAULT : (unsigned long long)ns;
     CUDA_OK(cudaMemcpyToSymbol(g_wait_ns, &v, sizeof(v)));
@@ -982,6 +1031,8 @@ extern "C" int qd_tc_set_wait_limit(long long ns) {
 
 extern "C" void qd_tc_work_free_on(struct QdTcWork *w, cudaStream_t st);
 
+// Work buffers of the tensor-core path (device), sized for an n x n matrix
+// and rank-2K updates with K <= kmax.
 struct QdTcWork {
     float *bx_hi, *bx_lo;  // 64 x pitch_x
     int64_t pitch_x;
@@ -1070,11 +1121,22 @@ extern "C" int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, i
     a.tiles_m = (m + TILE_M - 1) / TILE_M;
     a.tiles_n = 1;
     a.kblocks = (int)((2 * (int64_t)m + BKF - 1) / BKF);
-    int nsm = sm_count();
-    int splits = (2 * nsm + a.tiles_m - 1) / a.tiles_m;  // about two items per SM
-    if (splits > w->max_splits) splits = w->max_splits;
-    if (splits > a.kblocks) splits = a.kblocks;
-    if (splits < 1) splits = 1;
+    // Split-K count: the items (row tile, k range) are equal, so the grid of
+    // one CTA per SM finishes together when their count is just below a
+    // multiple of the SM count.  Pick the split with the best fill of the last
+    // wave (ties: fewer splits, fewer partials to reduce).
+    const int nsm = sm_count();
+    int splits = 1;
+    double best = -1.0;
+    for (int sp = 1; sp <= w->max_splits && sp <= a.kblocks; sp++) {
+        const long items = (long)a.tiles_m * sp;
+        const long waves = (items + nsm - 1) / nsm;
+        const double fill = (double)items / (double)(waves * nsm);
+        if (fill > best + 1e-3) {
+            best = fill;
+            splits = sp;
+        }
+    }
     a.splits = splits;
     a.n_items = a.tiles_m * splits;
     a.kdim = 0;
