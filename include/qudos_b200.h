@@ -140,6 +140,42 @@ void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coul
                              struct material_params *parameters, int *N_states,
                              struct eigenstate *eigenstate_vb, struct eigenstate *eigenstate_cb,
                              struct coulomb_matrix_element CME, int coulomb_region_type);
+
+/* Globals of the momentum-matrix-element stage (8_band.h): include_MME,
+ * Polarisation_Indicator (the polarisation whose dH/dk is current),
+ * Num_Possible_Polarisations, and the reference's host work arrays dH_dk and
+ * yV, which this library leaves unwritten (it keeps both on the device). */
+extern int include_MME, Polarisation_Indicator, Num_Possible_Polarisations;
+extern qd_complex128 *dH_dk, *yV;
+
+/* Replaces code/source/8_band/hamiltonian_derivative_8_band.c:23.  dH/dk
+ * along [100], [010] or [001] (polarisation 0, 1, 2) into the caller's host
+ * H_dk, lower triangle, leading dimension na_rows = N_H, from the same global
+ * coefficient tables as hamiltonian_8_band. */
+void hamiltonian_derivative_8_band(int polarisation, int N_shape, struct wave_vectors basis,
+                                   struct supercell_geometry *supercell, struct material_params *parameters,
+                                   qd_complex128 *H_dk);
+
+/* Replaces code/source/8_band/momentum_matrix_element.c:24: returns
+ * <psi_2| dH/dk_polarisation |psi_1> (eV Angstrom).  dH/dk is rebuilt on the
+ * device when Polarisation_Indicator differs from polarisation; dH/dk psi_1
+ * is recomputed when eigenstate_2_idx == 2 N_states[0] - 1 (the first valence
+ * state of the reference's loop, 8_band_main.c:1635-1655) and reused for the
+ * other valence states. */
+qd_complex128 momentum_matrix_element(int polarisation, int N_shape, struct wave_vectors basis,
+                                      struct supercell_geometry *supercell, struct material_params *parameters,
+                                      struct eigenstate eigenstate_1, int64_t eigenstate_1_idx,
+                                      struct eigenstate eigenstate_2, int64_t eigenstate_2_idx, int *N_states);
+
+/* Replaces code/source/8_band/envelope_functions.c:23.  For the 2 N_states[type]
+ * states of `eigenstate` (type 0 valence, 1 conduction) fills F_1..F_8 (the
+ * envelope of each Bloch band, sum_G a_G exp(i (G + K).r) / sqrt(L1 L2 L3))
+ * and probability_1..probability_8 = |F_b|^2, each caller-allocated with
+ * N_grid entries, at the points (x, y, z) in Angstrom; `direction` only names
+ * the scan for the output writers. */
+void envelope_functions(struct supercell_geometry *supercell, int *N_states, int type, int N_grid, double *x,
+                        double *y, double *z, struct wave_vectors basis, struct eigenstate *eigenstate,
+                        int direction);
 #endif /* QD_NO_REFERENCE_TYPES */
 
 /* ------------------------------------------------------------------------- */
@@ -168,6 +204,9 @@ typedef struct qd_problem qd_problem;
 int qd_problem_load(const char *dir, const char *const *overrides, int n_overrides, qd_problem **out);
 void qd_problem_free(qd_problem *pr);
 int qd_problem_n_shape(const qd_problem *pr);
+/* Applied field F (V/Angstrom) and Bloch wave vector K (1/Angstrom) of a
+ * loaded problem, in the units the reference's routines take them. */
+int qd_problem_field(const qd_problem *pr, double F[3], double K[3]);
 /* Number of libqdgpu kernel launches since the library was loaded (library
  * GEMMs from cuBLAS not included). */
 long long qd_launch_count(void);
@@ -215,6 +254,28 @@ int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *ei
 int qd_coulomb(qd_problem *pr, int n_vb_states, int n_cb_states, const qd_complex128 *eigvec_host,
                int madelung_ranks, qd_complex128 *hh, qd_complex128 *ee, qd_complex128 *eh_direct,
                qd_complex128 *eh_exchange);
+
+/* dH/dk_axis (axis 0, 1, 2: [100], [010], [001]) of a loaded problem on the
+ * device, complex128, lower triangle (mode 0) or full Hermitian (mode 1). */
+int qd_problem_assemble_dk_dev(qd_problem *pr, int axis, void *H_dev, int64_t ld, int mode, void *stream);
+
+/* Interband momentum matrix elements of a loaded problem (the loop of
+ * 8_band_main.c:1578-1680 over momentum_matrix_element.c:24): eigvec_host
+ * holds the window's states, n_vb_states valence states first (ascending)
+ * then n_cb_states conduction states, N_H each.
+ * mme[(pol * n_cb_states + c) * n_vb_states + v] = <vb_{n_vb_states-1-v}|
+ * dH/dk_pol |cb_c> in eV Angstrom (valence states counted from the highest,
+ * as the reference does).  All pairs of a polarisation come from one dH/dk
+ * assembled on the device, one product with the conduction states and one
+ * reduction. */
+int qd_momentum_matrix_elements(qd_problem *pr, const qd_complex128 *eigvec_host, int n_vb_states, int n_cb_states,
+                                qd_complex128 *mme);
+
+/* Real-space envelopes of m host states (N_H x m) of a loaded problem at
+ * n_grid points (x, y, z in Angstrom): F and prob (host, either may be NULL)
+ * receive [state][band][point] values of the band envelopes and of |F|^2. */
+int qd_envelope_functions(qd_problem *pr, const qd_complex128 *eigvec_host, int m, int n_grid, const double *x,
+                          const double *y, const double *z, qd_complex128 *F, double *prob);
 
 /* Device plumbing for callers without their own CUDA binding.  qd_memcpy kind:
  * 1 host->device, 2 device->host, 3 device->device.  Events time work on a

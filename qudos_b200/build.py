@@ -21,7 +21,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["tables.cu", "assemble.cu", "eig_stage1.cu", "eig_stage2.cu", "eig_driver.cu", "eig_refine.cu",
-              "panel_ops.cu", "coulomb.cu", "tc_gemm.cu"]
+              "panel_ops.cu", "envelope.cu", "coulomb.cu", "tc_gemm.cu"]
 C_SOURCES = ["host_inputs.c", "qd_api.c", "batch.c"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

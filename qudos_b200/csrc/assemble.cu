@@ -191,6 +191,56 @@ __device__ __forceinline__ void band_values(const Ctx &c, int64_t t, const doubl
     }
 }
 
+// Derivatives of the twelve band functions with respect to the Bloch wave
+// vector component K_ax (the momentum operator of the momentum matrix
+// elements, hamiltonian_derivative_8_band_matrix_elements.c:27-969).  The band
+// functions are polynomials of degree two in K, so with s = G1 + G2 + 2K the
+// derivative of every (G1 + K)_a (G2 + K)_b term is exact and constant terms
+// drop out.
+__device__ __forceinline__ void band_derivs(const Ctx &c, int64_t t, const double g1[3], const double g2[3], int ax,
+                                            zc (&v)[13]) {
+    const double K[3] = {c.K[0], c.K[1], c.K[2]};
+    double sv[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) sv[a] = g1[a] + g2[a] + 2.0 * K[a];
+    const double sx = sv[0], sy = sv[1], sz = sv[2], sa = sv[ax];
+    const double H2 = 0.5 * QD_HBSQM;
+    const zc f10 = ld(c, 10, t), f11 = ld(c, 11, t), P = ld(c, 12, t);
+    v[F_ZERO] = zc(0.0);
+    v[F_ECB] = H2 * ld(c, 1, t) * sa;
+    v[F_EHH] = -H2 * (ax < 2 ? ld(c, 3, t) : ld(c, 4, t)) * sa;
+    v[F_ELH] = -H2 * (ax < 2 ? ld(c, 6, t) : ld(c, 7, t)) * sa;
+    v[F_ESO] = -H2 * ld(c, 9, t) * sa;
+    v[F_Q] = (ax < 2 ? -sqrt(0.5) * QD_HBSQM : sqrt(2.0) * QD_HBSQM) * f10 * sa;
+    {
+        const double a = 0.5 * sqrt(3.0) * QD_HBSQM;
+        const zc kin = ax == 0 ? a * f10 * sx : ax == 1 ? -a * f10 * sy : zc(0.0);
+        const zc off = ax == 0 ? a * f11 * sy : ax == 1 ? a * f11 * sx : zc(0.0);
+        v[F_R] = kin - I_times(off);
+        v[F_RC] = kin + I_times(off);
+    }
+    {
+        const double a = 0.5 * sqrt(1.5) * QD_HBSQM;
+        const zc re = ax == 0 ? a * f11 * sz : ax == 2 ? a * f11 * sx : zc(0.0);
+        const zc im = ax == 1 ? a * f11 * sz : ax == 2 ? a * f11 * sy : zc(0.0);
+        v[F_S] = re - I_times(im);
+        v[F_SC] = re + I_times(im);
+    }
+    {
+        // d kx / d Kx = 2 for the linear terms in kx = G1x + G2x + 2 Kx
+        const zc Txx = ld(c, 22, t), Txy = ld(c, 23, t), Tyy = ld(c, 24, t), Txz = ld(c, 25, t), Tyz = ld(c, 26, t);
+        const double c6 = -0.5 / sqrt(6.0), i26 = 1.0 / (2.0 * sqrt(6.0)), c3 = -0.5 / sqrt(3.0);
+        const zc base = ax == 0 ? Txx : ax == 1 ? Txy : Txz;
+        const zc sI = ax == 0 ? Txy : ax == 1 ? Tyy : Tyz;
+        const zc p0 = ax == 0 ? 2.0 * i26 * P : zc(0.0);
+        const zc p1 = ax == 1 ? I_times(2.0 * i26 * P) : zc(0.0);
+        v[F_TP] = p0 + p1 + (2.0 * c6) * (base + I_times(sI));
+        v[F_TM] = p0 - p1 + (2.0 * c6) * (base - I_times(sI));
+        const zc tz = ax == 0 ? Txz : ax == 1 ? Tyz : ld(c, 27, t);
+        v[F_U] = (ax == 2 ? (2.0 / (2.0 * sqrt(3.0))) * P : zc(0.0)) + (2.0 * c3) * tz;
+    }
+}
+
 __device__ __forceinline__ int64_t diff_index(const Ctx &c, const int r[3], const int q[3]) {
     return ((int64_t)(r[0] - q[0] + c.NT[0] / 2) * c.NT[1] + (r[1] - q[1] + c.NT[1] / 2)) * c.NT[2] +
            (r[2] - q[2] + c.NT[2] / 2);
@@ -203,7 +253,8 @@ __device__ __forceinline__ int64_t diff_index(const Ctx &c, const int r[3], cons
 // hold 32 consecutive r for one q, so every store of a band block is 32
 // consecutive elements of one column.  Stores: complex128 into H64 (lower
 // triangle, or full with F64), complex64 into H32 (lower or full with F32).
-template <bool W64, bool F64, bool W32, bool F32>
+// DAX >= 0 writes dH/dK_DAX instead of H (same layout and symmetry).
+template <bool W64, bool F64, bool W32, bool F32, int DAX = -1>
 __global__ void __launch_bounds__(256) assemble_pw_kernel(Ctx c, int npw, double2 *__restrict__ H64, int64_t ld64,
                                                           float2 *__restrict__ H32, int64_t ld32) {
     const int r = blockIdx.x * 32 + threadIdx.x;
@@ -219,9 +270,14 @@ __global__ void __launch_bounds__(256) assemble_pw_kernel(Ctx c, int npw, double
         g2[a] = __ldg(&c.G[a][c.off[a] + iq[a]]);
     }
     zc v[13], u[13];
-    band_values(c, diff_index(c, ir, iq), g1, g2, v);
     constexpr bool need_upper = (W64 && F64) || (W32 && F32);
-    if (need_upper) band_values(c, diff_index(c, iq, ir), g2, g1, u);
+    if (DAX < 0) {
+        band_values(c, diff_index(c, ir, iq), g1, g2, v);
+        if (need_upper) band_values(c, diff_index(c, iq, ir), g2, g1, u);
+    } else {
+        band_derivs(c, diff_index(c, ir, iq), g1, g2, DAX, v);
+        if (need_upper) band_derivs(c, diff_index(c, iq, ir), g2, g1, DAX, u);
+    }
 #pragma unroll
     for (int cb = 0; cb < 8; cb++) {
 #pragma unroll
@@ -241,11 +297,11 @@ __global__ void __launch_bounds__(256) assemble_pw_kernel(Ctx c, int npw, double
     }
 }
 
-template <bool W64, bool F64, bool W32, bool F32>
+template <bool W64, bool F64, bool W32, bool F32, int DAX = -1>
 int launch_pw(const Ctx &c, int npw, double2 *H64, int64_t ld64, float2 *H32, int64_t ld32, cudaStream_t st) {
     dim3 grid((unsigned)((npw + 31) / 32), (unsigned)((npw + 7) / 8)), block(32, 8);
     qd_count_launch(1);
-    assemble_pw_kernel<W64, F64, W32, F32><<<grid, block, 0, st>>>(c, npw, H64, ld64, H32, ld32);
+    assemble_pw_kernel<W64, F64, W32, F32, DAX><<<grid, block, 0, st>>>(c, npw, H64, ld64, H32, ld32);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "assemble launch: %s", cudaGetErrorString(e));
     return QD_OK;
@@ -303,6 +359,37 @@ extern "C" int qd_assemble_launch(const void *d_coef, const double *d_Gx, const 
         return full ? launch_pw<false, false, true, true>(c, (int)npw, nullptr, 0, (float2 *)H, ld, st)
                     : launch_pw<false, false, true, false>(c, (int)npw, nullptr, 0, (float2 *)H, ld, st);
     return qd_set_error(QD_ERR_ARG, "unknown precision %d", prec);
+}
+
+// dH/dK_axis (axis 0, 1, 2), complex128, lower triangle (mode 0) or full
+// Hermitian (mode 1) into H (ld), from the problem's coefficient table.
+extern "C" int qd_assemble_dk_launch(const void *d_coef, const double *d_Gx, const double *d_Gy, const double *d_Gz,
+                                     const int N[3], const double K[3], int axis, void *H, int64_t ld, int mode,
+                                     void *stream) {
+    if (upload_block_map() != QD_OK) return qd_set_error(QD_ERR_CUDA, "block map upload failed");
+    if (axis < 0 || axis > 2) return qd_set_error(QD_ERR_ARG, "derivative axis %d not in 0..2", axis);
+    Ctx c;
+    c.coef = (const double2 *)d_coef;
+    c.G[0] = d_Gx; c.G[1] = d_Gy; c.G[2] = d_Gz;
+    for (int a = 0; a < 3; a++) {
+        c.N[a] = N[a];
+        c.NT[a] = 2 * N[a] - 1;
+        c.off[a] = c.NT[a] / 2 - N[a] / 2;
+        c.K[a] = K[a];
+    }
+    c.nT = (int64_t)c.NT[0] * c.NT[1] * c.NT[2];
+    const int64_t npw = (int64_t)N[0] * N[1] * N[2];
+    if (ld < 8 * npw) return qd_set_error(QD_ERR_ARG, "leading dimension below N_H");
+    cudaStream_t st = (cudaStream_t)stream;
+    double2 *Hd = (double2 *)H;
+    if (mode == 1) {
+        if (axis == 0) return launch_pw<true, true, false, false, 0>(c, (int)npw, Hd, ld, nullptr, 0, st);
+        if (axis == 1) return launch_pw<true, true, false, false, 1>(c, (int)npw, Hd, ld, nullptr, 0, st);
+        return launch_pw<true, true, false, false, 2>(c, (int)npw, Hd, ld, nullptr, 0, st);
+    }
+    if (axis == 0) return launch_pw<true, false, false, false, 0>(c, (int)npw, Hd, ld, nullptr, 0, st);
+    if (axis == 1) return launch_pw<true, false, false, false, 1>(c, (int)npw, Hd, ld, nullptr, 0, st);
+    return launch_pw<true, false, false, false, 2>(c, (int)npw, Hd, ld, nullptr, 0, st);
 }
 
 // Both copies in one pass: complex128 into H64 and complex64 into H32 (same ld).

@@ -36,6 +36,11 @@ QD_WEAK struct strain_tensor strain_G = {0};
 QD_WEAK struct convolution_char_strain *convolutions_char_strain = NULL;
 QD_WEAK struct piezo_potential phi_piezo_G = {0};
 QD_WEAK struct timing component_run_times = {0};
+QD_WEAK int include_MME = 0;
+QD_WEAK int Polarisation_Indicator = -1;
+QD_WEAK int Num_Possible_Polarisations = 3;
+QD_WEAK qd_complex128 *dH_dk = NULL;
+QD_WEAK qd_complex128 *yV = NULL;
 
 /* ------------------------------------------------------------------------- */
 /* errors                                                                    */
@@ -324,6 +329,15 @@ void qd_problem_free(qd_problem *pr) {
     free(pr);
 }
 
+int qd_problem_field(const qd_problem *pr, double F[3], double K[3]) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    for (int a = 0; a < 3; a++) {
+        if (F) F[a] = pr->p.F[a];
+        if (K) K[a] = pr->p.K[a];
+    }
+    return QD_OK;
+}
+
 int qd_problem_n_shape(const qd_problem *pr) { return pr ? pr->p.n_shape : 0; }
 
 int qd_problem_sizes(const qd_problem *pr, int64_t *n_pw, int64_t *n_h, int *lo, int *hi, int *n_vb, int *n_cb) {
@@ -454,7 +468,7 @@ static int check_single_rank(void) {
 /* Uploads the reference's global tables, fuses them and assembles H on the device. */
 static int assemble_from_globals(int n_shape, struct vector F, struct wave_vectors basis,
                                  struct supercell_geometry *supercell, struct material_params *parameters, void *H_dev,
-                                 int64_t ld) {
+                                 int64_t ld, int dk_axis) {
     int N[3] = {basis.N_Gx, basis.N_Gy, basis.N_Gz};
     const qd_complex128 *chi[1024];
     const qd_complex128 *eps[6];
@@ -485,7 +499,10 @@ static int assemble_from_globals(int n_shape, struct vector F, struct wave_vecto
     if (rc) return rc;
     int NT[3] = {2 * N[0] - 1, 2 * N[1] - 1, 2 * N[2] - 1};
     double K[3] = {basis.Kx, basis.Ky, basis.Kz};
-    rc = qd_assemble_launch(d_coef, d_G, d_G + NT[0], d_G + NT[0] + NT[1], N, K, H_dev, ld, 0, QD_PREC_FP64, NULL);
+    rc = dk_axis < 0 ? qd_assemble_launch(d_coef, d_G, d_G + NT[0], d_G + NT[0] + NT[1], N, K, H_dev, ld, 0,
+                                          QD_PREC_FP64, NULL)
+                     : qd_assemble_dk_launch(d_coef, d_G, d_G + NT[0], d_G + NT[0] + NT[1], N, K, dk_axis, H_dev, ld,
+                                             0, NULL);
     if (rc == QD_OK && cudaDeviceSynchronize() != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "assembly failed");
     cudaFree(d_coef);
     cudaFree(d_G);
@@ -500,7 +517,7 @@ void hamiltonian_8_band(int n_shape, struct vector F, struct wave_vectors basis,
     void *Hd = NULL;
     if (rc == QD_OK && qd_pool_alloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n, NULL) != 0)
         rc = qd_set_error(QD_ERR_NOMEM, "device H");
-    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, ld);
+    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, ld, -1);
     /* copy the lower triangle column by column; the caller's strict upper triangle is left as it was */
     for (int64_t c = 0; rc == QD_OK && c < n; c++) {
         cudaError_t e = cudaMemcpy(H + c + c * ld, (qd_complex128 *)Hd + c + c * ld, sizeof(qd_complex128) * (size_t)(n - c),
@@ -548,7 +565,7 @@ void eigenstates(int n_shape, int *N_states, struct vector F, struct wave_vector
                         qd_pool_alloc((void **)&wd, sizeof(double) * (size_t)M, NULL) != 0))
         rc = qd_set_error(QD_ERR_NOMEM, "device buffers");
     double t0 = wall_s();
-    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, n);
+    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F, basis, supercell, parameters, Hd, n, -1);
     double t1 = wall_s();
     if (rc == QD_OK) rc = qd_eigh_window(n, Hd, n, lo, hi, env_precision(), wd, Zd, n, NULL);
     double t2 = wall_s();
@@ -734,4 +751,242 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i]) qd_pool_free(bufs[i], NULL);
     return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Momentum matrix elements <vb| dH/dk_a |cb>                                 */
+/* ------------------------------------------------------------------------- */
+int qd_problem_assemble_dk_dev(qd_problem *pr, int axis, void *H_dev, int64_t ld, int mode, void *stream) {
+    if (!pr) return qd_set_error(QD_ERR_ARG, "null problem");
+    RC(qd_problem_build_tables(pr));
+    return qd_assemble_dk_launch(pr->d_coef, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, axis, H_dev, ld,
+                                 mode, stream);
+}
+
+int qd_momentum_matrix_elements(qd_problem *pr, const qd_complex128 *eigvec_host, int n_vb_states, int n_cb_states,
+                                qd_complex128 *mme) {
+    if (!pr || !eigvec_host || !mme || n_vb_states < 1 || n_cb_states < 1)
+        return qd_set_error(QD_ERR_ARG, "qd_momentum_matrix_elements: bad arguments");
+    RC(qd_problem_build_tables(pr));
+    const int64_t n = pr->n_h;
+    const int M = n_vb_states + n_cb_states;
+    void *dH = NULL, *Z = NULL, *Y = NULL, *G = NULL;
+    int rc = QD_OK;
+    if (qd_pool_alloc(&dH, sizeof(qd_complex128) * (size_t)n * (size_t)n, NULL) ||
+        qd_pool_alloc(&Z, sizeof(qd_complex128) * (size_t)n * M, NULL) ||
+        qd_pool_alloc(&Y, sizeof(qd_complex128) * (size_t)n * n_cb_states, NULL) ||
+        qd_pool_alloc(&G, sizeof(qd_complex128) * (size_t)n_vb_states * n_cb_states, NULL))
+        rc = qd_set_error(QD_ERR_NOMEM, "qd_momentum_matrix_elements: device buffers");
+    if (rc == QD_OK && cudaMemcpy(Z, eigvec_host, sizeof(qd_complex128) * (size_t)n * M, cudaMemcpyHostToDevice) !=
+                           cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "qd_momentum_matrix_elements: upload");
+    qd_complex128 *g = (qd_complex128 *)malloc(sizeof(qd_complex128) * (size_t)n_vb_states * n_cb_states);
+    if (rc == QD_OK && !g) rc = qd_set_error(QD_ERR_NOMEM, "qd_momentum_matrix_elements");
+    const qd_complex128 *Zcb = (const qd_complex128 *)Z + (size_t)n * n_vb_states;
+    for (int a = 0; rc == QD_OK && a < 3; a++) {
+        /* momentum_matrix_element.c:81 (zhemv) and :97 (zdotc), all pairs at once */
+        if ((rc = qd_problem_assemble_dk_dev(pr, a, dH, n, 0, NULL))) break;
+        if ((rc = qd_hemm_lower_dev(n, dH, n, Zcb, n, n_cb_states, Y, n, 0.0, NULL))) break;
+        if ((rc = qd_gram_dev(n, Z, n, n_vb_states, Y, n, n_cb_states, G, n_vb_states, NULL))) break;
+        if (cudaMemcpy(g, G, sizeof(qd_complex128) * (size_t)n_vb_states * n_cb_states, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+            rc = qd_set_error(QD_ERR_CUDA, "qd_momentum_matrix_elements: copy-out");
+            break;
+        }
+        /* 8_band_main.c:1647: [pol][cb][vb], valence states from the highest down */
+        for (int c = 0; c < n_cb_states; c++)
+            for (int v = 0; v < n_vb_states; v++)
+                mme[((size_t)a * n_cb_states + c) * n_vb_states + v] = g[(n_vb_states - 1 - v) + (size_t)c * n_vb_states];
+    }
+    free(g);
+    void *bufs[] = {dH, Z, Y, G};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        if (bufs[i]) qd_pool_free(bufs[i], NULL);
+    return rc;
+}
+
+/* Replaces code/source/8_band/hamiltonian_derivative_8_band.c:23: dH/dk for
+ * polarisation 0, 1, 2 ([100], [010], [001]) into the caller's host H_dk
+ * (lower triangle, leading dimension na_rows), from the reference's globals. */
+void hamiltonian_derivative_8_band(int polarisation, int n_shape, struct wave_vectors basis,
+                                   struct supercell_geometry *supercell, struct material_params *parameters,
+                                   qd_complex128 *H_dk) {
+    int rc = check_single_rank();
+    int64_t n = (int64_t)8 * basis.N_Gx * basis.N_Gy * basis.N_Gz;
+    int64_t ld = na_rows > 0 ? na_rows : n;
+    void *Hd = NULL;
+    if (rc == QD_OK && qd_pool_alloc(&Hd, sizeof(qd_complex128) * (size_t)ld * (size_t)n, NULL) != 0)
+        rc = qd_set_error(QD_ERR_NOMEM, "device dH/dk");
+    struct vector F0 = {0.0, 0.0, 0.0};
+    if (rc == QD_OK) rc = assemble_from_globals(n_shape, F0, basis, supercell, parameters, Hd, ld, polarisation);
+    for (int64_t c = 0; rc == QD_OK && c < n; c++) {
+        cudaError_t e = cudaMemcpy(H_dk + c + c * ld, (qd_complex128 *)Hd + c + c * ld,
+                                   sizeof(qd_complex128) * (size_t)(n - c), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "copy-out: %s", cudaGetErrorString(e));
+    }
+    if (Hd) qd_pool_free(Hd, NULL);
+    if (rc) die("hamiltonian_derivative_8_band", rc);
+}
+
+/* Device state of momentum_matrix_element between calls: dH/dk of the
+ * current polarisation (Polarisation_Indicator), the product y = dH/dk psi_1
+ * of the last conduction state and a staging vector for psi_2. */
+static struct {
+    void *dH, *psi, *y, *r;
+    int64_t n;
+    int pol;
+} g_mme = {NULL, NULL, NULL, NULL, 0, -1};
+
+/* Replaces code/source/8_band/momentum_matrix_element.c:24.  Same contract:
+ * dH/dk is rebuilt when Polarisation_Indicator differs from polarisation,
+ * y = dH/dk psi_1 is recomputed when eigenstate_2_idx is the first valence
+ * state (2 N_states[0] - 1) and otherwise reused, and the result is
+ * psi_2^H y.  dH/dk and y stay on the device; the reference's host arrays
+ * dH_dk and yV are not written. */
+qd_complex128 momentum_matrix_element(int polarisation, int n_shape, struct wave_vectors basis,
+                                      struct supercell_geometry *supercell, struct material_params *parameters,
+                                      struct eigenstate eigenstate_1, int64_t eigenstate_1_idx,
+                                      struct eigenstate eigenstate_2, int64_t eigenstate_2_idx, int *N_states) {
+    (void)eigenstate_1_idx;
+    int rc = check_single_rank();
+    const int64_t n = (int64_t)8 * basis.N_Gx * basis.N_Gy * basis.N_Gz;
+    if (rc == QD_OK && g_mme.n != n) {
+        void *p[] = {g_mme.dH, g_mme.psi, g_mme.y, g_mme.r};
+        for (int i = 0; i < 4; i++)
+            if (p[i]) cudaFree(p[i]);
+        g_mme.dH = g_mme.psi = g_mme.y = g_mme.r = NULL;
+        if (cudaMalloc(&g_mme.dH, sizeof(qd_complex128) * (size_t)n * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&g_mme.psi, sizeof(qd_complex128) * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&g_mme.y, sizeof(qd_complex128) * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&g_mme.r, sizeof(qd_complex128)) != cudaSuccess)
+            rc = qd_set_error(QD_ERR_NOMEM, "momentum_matrix_element: device buffers");
+        g_mme.n = rc == QD_OK ? n : 0;
+        g_mme.pol = -1;
+        Polarisation_Indicator = -1;
+    }
+    if (rc == QD_OK && (Polarisation_Indicator != polarisation || g_mme.pol != polarisation)) {
+        struct vector F0 = {0.0, 0.0, 0.0};
+        rc = assemble_from_globals(n_shape, F0, basis, supercell, parameters, g_mme.dH, n, polarisation);
+        if (rc == QD_OK) {
+            Polarisation_Indicator = polarisation;
+            g_mme.pol = polarisation;
+        }
+    }
+    if (rc == QD_OK && eigenstate_2_idx == 2 * (int64_t)N_states[0] - 1) {
+        if (cudaMemcpy(g_mme.psi, eigenstate_1.fourier, sizeof(qd_complex128) * (size_t)n, cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            rc = qd_set_error(QD_ERR_CUDA, "momentum_matrix_element: upload");
+        if (rc == QD_OK) rc = qd_hemm_lower_dev(n, g_mme.dH, n, g_mme.psi, n, 1, g_mme.y, n, 0.0, NULL);
+    }
+    qd_complex128 result;
+    memset(&result, 0, sizeof(result));
+    if (rc == QD_OK &&
+        cudaMemcpy(g_mme.psi, eigenstate_2.fourier, sizeof(qd_complex128) * (size_t)n, cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "momentum_matrix_element: upload");
+    if (rc == QD_OK) rc = qd_gram_dev(n, g_mme.psi, n, 1, g_mme.y, n, 1, g_mme.r, 1, NULL);
+    if (rc == QD_OK && cudaMemcpy(&result, g_mme.r, sizeof(result), cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "momentum_matrix_element: copy-out");
+    if (rc) die("momentum_matrix_element", rc);
+    return result;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Real-space envelope functions (envelope_functions.c:23-220)                */
+/* ------------------------------------------------------------------------- */
+int qd_envelope_dev(const int N[3], const double *d_Gx, const double *d_Gy, const double *d_Gz, const double K[3],
+                    double volume, const void *Z, int64_t ldz, int m, int n_grid, const double *x, const double *y,
+                    const double *z, void *F, double *prob, void *stream);
+
+/* Host-side driver shared by the qd_ entry point and the reference-named one:
+ * G grids and points are host arrays, states host N_H x m; outputs host
+ * [state][band][point] (either may be NULL). */
+static int envelopes_host(const int N[3], const double *const G[3], const double K[3], double volume,
+                          const qd_complex128 *Zh, int64_t ldz, int m, int n_grid, const double *x, const double *y,
+                          const double *z, qd_complex128 *F, double *prob) {
+    const int64_t npw = (int64_t)N[0] * N[1] * N[2], nh = 8 * npw;
+    const int NT[3] = {2 * N[0] - 1, 2 * N[1] - 1, 2 * N[2] - 1};
+    double *dG = NULL, *dp = NULL, *dprob = NULL;
+    void *dZ = NULL, *dF = NULL;
+    int rc = QD_OK;
+    const size_t nout = (size_t)m * 8 * n_grid;
+    if (cudaMalloc((void **)&dG, sizeof(double) * (NT[0] + NT[1] + NT[2])) != cudaSuccess ||
+        cudaMalloc((void **)&dp, sizeof(double) * 3 * (size_t)n_grid) != cudaSuccess ||
+        cudaMalloc(&dZ, sizeof(qd_complex128) * (size_t)nh * m) != cudaSuccess ||
+        (F && cudaMalloc(&dF, sizeof(qd_complex128) * nout) != cudaSuccess) ||
+        (prob && cudaMalloc((void **)&dprob, sizeof(double) * nout) != cudaSuccess))
+        rc = qd_set_error(QD_ERR_NOMEM, "envelope functions: device buffers");
+    for (int a = 0, o = 0; rc == QD_OK && a < 3; o += NT[a], a++)
+        if (cudaMemcpy(dG + o, G[a], sizeof(double) * NT[a], cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = qd_set_error(QD_ERR_CUDA, "envelope functions: upload");
+    if (rc == QD_OK && (cudaMemcpy(dp, x, sizeof(double) * n_grid, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dp + n_grid, y, sizeof(double) * n_grid, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dp + 2 * (size_t)n_grid, z, sizeof(double) * n_grid, cudaMemcpyHostToDevice) !=
+                            cudaSuccess ||
+                        cudaMemcpy2D(dZ, sizeof(qd_complex128) * nh, Zh, sizeof(qd_complex128) * ldz,
+                                     sizeof(qd_complex128) * nh, m, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = qd_set_error(QD_ERR_CUDA, "envelope functions: upload");
+    if (rc == QD_OK)
+        rc = qd_envelope_dev(N, dG, dG + NT[0], dG + NT[0] + NT[1], K, volume, dZ, nh, m, n_grid, dp, dp + n_grid,
+                             dp + 2 * (size_t)n_grid, dF, dprob, NULL);
+    if (rc == QD_OK && F && cudaMemcpy(F, dF, sizeof(qd_complex128) * nout, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "envelope functions: copy-out");
+    if (rc == QD_OK && prob && cudaMemcpy(prob, dprob, sizeof(double) * nout, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = qd_set_error(QD_ERR_CUDA, "envelope functions: copy-out");
+    cudaFree(dG);
+    cudaFree(dp);
+    cudaFree(dZ);
+    cudaFree(dF);
+    cudaFree(dprob);
+    return rc;
+}
+
+int qd_envelope_functions(qd_problem *pr, const qd_complex128 *eigvec_host, int m, int n_grid, const double *x,
+                          const double *y, const double *z, qd_complex128 *F, double *prob) {
+    if (!pr || !eigvec_host || m < 1 || n_grid < 1 || !x || !y || !z)
+        return qd_set_error(QD_ERR_ARG, "qd_envelope_functions: bad arguments");
+    const double vol = pr->geo[0].L1 * pr->geo[0].L2 * pr->geo[0].L3;
+    const double *G[3] = {pr->G[0], pr->G[1], pr->G[2]};
+    return envelopes_host(pr->p.N, G, pr->p.K, vol, eigvec_host, pr->n_h, m, n_grid, x, y, z, F, prob);
+}
+
+/* Replaces code/source/8_band/envelope_functions.c:23.  For the 2 N_states[type]
+ * states of eigenstate (type 0 valence, 1 conduction) fills F_1..F_8 and
+ * probability_1..probability_8 (caller-allocated, N_grid each) at the points
+ * (x, y, z) in Angstrom.  `direction` only names the scan for the writers. */
+void envelope_functions(struct supercell_geometry *supercell, int *N_states, int type, int N_grid, double *x,
+                        double *y, double *z, struct wave_vectors basis, struct eigenstate *eigenstate,
+                        int direction) {
+    (void)direction;
+    int rc = check_single_rank();
+    const int m = 2 * N_states[type];
+    const int N[3] = {basis.N_Gx, basis.N_Gy, basis.N_Gz};
+    const int64_t nh = (int64_t)8 * N[0] * N[1] * N[2];
+    const double *G[3] = {basis.Gx, basis.Gy, basis.Gz};
+    const double K[3] = {basis.Kx, basis.Ky, basis.Kz};
+    const double vol = supercell[0].L1 * supercell[0].L2 * supercell[0].L3;
+    qd_complex128 *Z = NULL, *F = NULL;
+    double *prob = NULL;
+    const size_t nout = (size_t)m * 8 * N_grid;
+    if (rc == QD_OK && (!(Z = (qd_complex128 *)malloc(sizeof(qd_complex128) * (size_t)nh * m)) ||
+                        !(F = (qd_complex128 *)malloc(sizeof(qd_complex128) * nout)) ||
+                        !(prob = (double *)malloc(sizeof(double) * nout))))
+        rc = qd_set_error(QD_ERR_NOMEM, "envelope_functions: host buffers");
+    for (int s = 0; rc == QD_OK && s < m; s++) memcpy(Z + (size_t)s * nh, eigenstate[s].fourier, sizeof(qd_complex128) * nh);
+    if (rc == QD_OK) rc = envelopes_host(N, G, K, vol, Z, nh, m, N_grid, x, y, z, F, prob);
+    for (int s = 0; rc == QD_OK && s < m; s++) {
+        qd_complex128 *Fb[8] = {eigenstate[s].F_1, eigenstate[s].F_2, eigenstate[s].F_3, eigenstate[s].F_4,
+                                eigenstate[s].F_5, eigenstate[s].F_6, eigenstate[s].F_7, eigenstate[s].F_8};
+        double *Pb[8] = {eigenstate[s].probability_1, eigenstate[s].probability_2, eigenstate[s].probability_3,
+                         eigenstate[s].probability_4, eigenstate[s].probability_5, eigenstate[s].probability_6,
+                         eigenstate[s].probability_7, eigenstate[s].probability_8};
+        for (int b = 0; b < 8; b++) {
+            if (Fb[b]) memcpy(Fb[b], F + ((size_t)s * 8 + b) * N_grid, sizeof(qd_complex128) * N_grid);
+            if (Pb[b]) memcpy(Pb[b], prob + ((size_t)s * 8 + b) * N_grid, sizeof(double) * N_grid);
+        }
+    }
+    free(Z);
+    free(F);
+    free(prob);
+    if (rc) die("envelope_functions", rc);
 }

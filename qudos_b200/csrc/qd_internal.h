@@ -78,6 +78,13 @@ int qd_assemble_launch(const void *d_coef, const double *d_Gx, const double *d_G
                        const int N[3], const double K[3], void *H, int64_t ld, int mode, int prec,
                        void *stream);
 
+int qd_assemble_dk_launch(const void *d_coef, const double *d_Gx, const double *d_Gy, const double *d_Gz,
+                          const int N[3], const double K[3], int axis, void *H, int64_t ld, int mode, void *stream);
+int qd_hemm_lower_dev(int64_t n, const void *H, int64_t ld, const void *X, int64_t ldx, int k, void *Y, int64_t ldy,
+                      double beta, void *stream);
+int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb, void *C, int ldc,
+                void *stream);
+
 /* eigensolver (eig.cu) */
 int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, int prec, double *w_dev,
                    void *Z_dev, int64_t ldz, void *stream);

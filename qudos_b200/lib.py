@@ -81,6 +81,10 @@ _sig("qd_version", ci, [])
 _sig("qd_problem_load", ci, [C.c_char_p, C.POINTER(C.c_char_p), ci, C.POINTER(vp)])
 _sig("qd_problem_free", None, [vp])
 _sig("qd_problem_n_shape", ci, [vp])
+_sig("qd_problem_field", ci, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)])
+_sig("qd_problem_assemble_dk_dev", ci, [vp, ci, vp, i64, ci, vp])
+_sig("qd_momentum_matrix_elements", ci, [vp, vp, ci, ci, vp])
+_sig("qd_envelope_functions", ci, [vp, vp, ci, ci, vp, vp, vp, vp, vp])
 _sig("qd_launch_count", C.c_longlong, [])
 _sig("qd_problem_sizes", ci, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(ci), C.POINTER(ci), C.POINTER(ci),
                               C.POINTER(ci)])
@@ -140,6 +144,22 @@ _sig("hamiltonian_8_band", None, [ci, Vector, WaveVectors, C.POINTER(SupercellGe
 _sig("diagonalise_hamiltonian", None, [C.POINTER(ci), vp, vp, vp])
 _sig("eigenstates", None, [ci, C.POINTER(ci), Vector, WaveVectors, C.POINTER(SupercellGeometry),
                            C.POINTER(MaterialParams), C.POINTER(Eigenstate), C.POINTER(Eigenstate)])
+
+
+class Complex128(C.Structure):
+    """A C double _Complex returned by value (two doubles, returned in SSE registers on x86-64)."""
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+_sig("hamiltonian_derivative_8_band", None, [ci, WaveVectors, C.POINTER(SupercellGeometry), C.POINTER(MaterialParams),
+                                             vp])
+_sig("momentum_matrix_element", Complex128, [ci, ci, WaveVectors, C.POINTER(SupercellGeometry),
+                                             C.POINTER(MaterialParams), Eigenstate, C.c_int64, Eigenstate, C.c_int64,
+                                             C.POINTER(ci)])
+
+
+_sig("envelope_functions", None, [C.POINTER(SupercellGeometry), C.POINTER(ci), ci, ci, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), WaveVectors, C.POINTER(Eigenstate), ci])
 
 
 def device_count():

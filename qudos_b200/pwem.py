@@ -81,6 +81,46 @@ class Problem:
         L.check(L.lib.qd_problem_solve(self._h, prec, w.ctypes.data, v.ctypes.data))
         return w, v
 
+    def field(self):
+        """(F in V/Angstrom, K in 1/Angstrom) as the reference's routines take them."""
+        F, K = (C.c_double * 3)(), (C.c_double * 3)()
+        L.check(L.lib.qd_problem_field(self._h, F, K))
+        return tuple(F), tuple(K)
+
+    def momentum(self, v, n_vb_states, n_cb_states):
+        """Interband momentum matrix elements (8_band_main.c:1578-1680):
+        p[pol, c, v] = <vb_(n_vb_states-1-v)| dH/dk_pol |cb_c> in eV Angstrom, pol
+        0, 1, 2 = [100], [010], [001]; v holds the VB states first."""
+        v = np.asfortranarray(v, dtype=np.complex128)
+        out = np.zeros((3, n_cb_states, n_vb_states), dtype=np.complex128)
+        L.check(L.lib.qd_momentum_matrix_elements(self._h, v.ctypes.data, n_vb_states, n_cb_states,
+                                                  out.ctypes.data))
+        return out
+
+    def envelopes(self, v, x, y, z):
+        """Band envelopes F (states, 8, points) and |F|^2 of the states v
+        (N_H x M) at the points x, y, z (Angstrom), envelope_functions.c:23."""
+        v = np.asfortranarray(v, dtype=np.complex128)
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        m, n = v.shape[1], len(x)
+        F = np.zeros((m, 8, n), dtype=np.complex128)
+        P = np.zeros((m, 8, n))
+        L.check(L.lib.qd_envelope_functions(self._h, v.ctypes.data, m, n, x.ctypes.data, y.ctypes.data,
+                                            z.ctypes.data, F.ctypes.data, P.ctypes.data))
+        return F, P
+
+    def assemble_dk(self, axis, mode=0):
+        """dH/dk_axis on the device, copied back (column-major N_H x N_H complex128)."""
+        n = self.n_h
+        buf = L.DeviceBuffer(n * n * 16)
+        L.check(L.lib.qd_memset(buf.ptr, 0, n * n * 16))
+        L.check(L.lib.qd_problem_assemble_dk_dev(self._h, axis, buf.ptr, n, mode, None))
+        L.check(L.lib.qd_device_synchronize())
+        H = np.empty((n, n), dtype=np.complex128, order="F")
+        buf.download(H)
+        buf.free()
+        return H
+
     def residuals(self, w, v):
         """FP64 check of eigenpairs against this problem's H, assembled on the
         device: (||H v_j - w_j v_j|| per state in eV, max |V^H V - I|, max |H_ij|)."""
@@ -154,6 +194,51 @@ def solve_batch(problems, prec=L.QD_PREC_MIXED, n_threads=8):
 
 def eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream=None):
     L.check(L.lib.qd_eigh_window_dev(n, H_dev, ld, lo, hi, prec, w_dev, Z_dev, ldz, stream))
+
+
+def write_momentum_matrix_elements(directory, mme):
+    """momentum_matrix_elements.dat as write_momentum_matrix_elements.c:23-110
+    writes it: per (CB state, VB state) row the 1-based indices, then Re, Im
+    and |.| of the element for [100], [010], [001], [110] = (p_x + p_y)/sqrt 2
+    and [-110] = (-p_x + p_y)/sqrt 2, divided by sqrt(HBSQM / 2) (eV^(1/2));
+    a blank line after each CB state."""
+    hb = np.sqrt(7.61996 / 2.0)
+    n_pol, ncb, nvb = mme.shape
+    with open(os.path.join(directory, "momentum_matrix_elements.dat"), "w") as f:
+        for c in range(ncb):
+            for v in range(nvb):
+                px, py, pz = mme[0, c, v] / hb, mme[1, c, v] / hb, mme[2, c, v] / hb
+                f.write("%d\t%d\t" % (c + 1, v + 1))
+                for z in (px, py, pz, (px + py) / np.sqrt(2.0), (-px + py) / np.sqrt(2.0)):
+                    f.write("%17.10e\t%17.10e\t%17.10e\t" % (z.real, z.imag, abs(z)))
+                f.write("\n")
+            f.write("\n")
+
+
+LINESCAN_TAGS = ("100", "010", "001", "110", "101", "011", "111")
+
+
+def write_probability_density(directory, direction, x, y, z, E_vb, prob_vb, E_cb, prob_cb):
+    """probability_density_{vb,cb}_<k>_<dir>.dat as write_probability_density.c
+    writes them (x, y, z in nm, energy, total / SO / LH / HH / CB densities in
+    nm^-3); VB files count from the highest state.  prob_* are (states, 8,
+    points) |F_b|^2 from Problem.envelopes; x, y, z in Angstrom."""
+    tag = LINESCAN_TAGS[direction]
+
+    def rows(E, p):
+        p = 1000.0 * p
+        return np.stack([0.1 * np.asarray(x), 0.1 * np.asarray(y), 0.1 * np.asarray(z), np.full(len(x), E),
+                         p.sum(axis=0), p[3] + p[7], p[2] + p[6], p[1] + p[5], p[0] + p[4]], axis=1)
+
+    fmt = "\t".join(["%13e"] * 9) + "\n"
+    nv = len(E_vb)
+    for k in range(nv):
+        s = nv - 1 - k
+        with open(os.path.join(directory, "probability_density_vb_%d_%s.dat" % (k + 1, tag)), "w") as f:
+            f.writelines(fmt % tuple(r) for r in rows(E_vb[s], prob_vb[s]))
+    for k in range(len(E_cb)):
+        with open(os.path.join(directory, "probability_density_cb_%d_%s.dat" % (k + 1, tag)), "w") as f:
+            f.writelines(fmt % tuple(r) for r in rows(E_cb[k], prob_cb[k]))
 
 
 def write_energies(directory, rows_vb, rows_cb):

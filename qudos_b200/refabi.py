@@ -84,7 +84,8 @@ class ReferenceCall:
         eps = [pr.table(1, c, 0, shp) for c in range(6)]
         phi = pr.table(2, 0, 0, shp)
         conv = [None] + [[pr.table(3, s, c, shp) for c in range(8)] for s in range(1, ns)]
-        return cls((N, N, N), geo, mat, chi, eps, conv, phi)
+        F, K = pr.field()
+        return cls((N, N, N), geo, mat, chi, eps, conv, phi, F=F, K=K)
 
     def _install(self):
         lib = L.lib
@@ -150,6 +151,56 @@ class ReferenceCall:
         E = np.array([vb[i].E for i in range(2 * n_vb)] + [cb[i].E for i in range(2 * n_cb)])
         self._states = (vb, cb, v)
         return E, v
+
+    def hamiltonian_derivative(self, polarisation):
+        """hamiltonian_derivative_8_band into a zeroed host array (lower triangle)."""
+        self._install()
+        H = np.zeros((self.n_h, self.n_h), dtype=np.complex128, order="F")
+        L.lib.hamiltonian_derivative_8_band(polarisation, self.n_shape, self.basis, self.gstruct, self.mstruct,
+                                            H.ctypes.data)
+        return H
+
+    def momentum_matrix_elements(self, v, n_vb, n_cb):
+        """The reference's loop (8_band_main.c:1632-1655) over momentum_matrix_element:
+        returns p[pol, c, v] for the states v (VB first), valence states from the highest down."""
+        self._install()
+        C.c_int.in_dll(L.lib, "Polarisation_Indicator").value = -1
+        v = np.asfortranarray(v, dtype=np.complex128)
+        nv, nc = 2 * n_vb, 2 * n_cb
+        states = (L.Eigenstate * (nv + nc))()
+        for i in range(nv + nc):
+            states[i].fourier = v[:, i].ctypes.data
+        nstates = (C.c_int * 2)(n_vb, n_cb)
+        out = np.zeros((3, nc, nv), dtype=np.complex128)
+        for pol in range(3):
+            for c in range(nc):
+                for iv in range(nv):
+                    j = nv - 1 - iv
+                    r = L.lib.momentum_matrix_element(pol, self.n_shape, self.basis, self.gstruct, self.mstruct,
+                                                      states[nv + c], nv + c, states[j], j, nstates)
+                    out[pol, c, iv] = r.re + 1j * r.im
+        return out
+
+    def envelope_functions(self, v, N_states, kind, x, y, z, direction=0):
+        """envelope_functions() for the 2 N_states[kind] states v (kind 0 valence,
+        1 conduction): the caller allocates F_1..F_8 and probability_1..8 of
+        every state (8_band_main.c:824-893); returns (F, prob) as (states, 8, points)."""
+        v = np.asfortranarray(v, dtype=np.complex128)
+        m, n = v.shape[1], len(x)
+        F = np.zeros((m, 8, n), dtype=np.complex128)
+        P = np.zeros((m, 8, n))
+        st = (L.Eigenstate * m)()
+        for s in range(m):
+            st[s].fourier = v[:, s].ctypes.data
+            for b in range(8):
+                setattr(st[s], "F_%d" % (b + 1), F[s, b].ctypes.data)
+                setattr(st[s], "probability_%d" % (b + 1), P[s, b].ctypes.data_as(C.POINTER(C.c_double)))
+        xs, ys, zs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        ns = (C.c_int * 2)(*N_states)
+        dp = C.POINTER(C.c_double)
+        L.lib.envelope_functions(self.gstruct, ns, kind, n, xs.ctypes.data_as(dp), ys.ctypes.data_as(dp),
+                                 zs.ctypes.data_as(dp), self.basis, st, direction)
+        return F, P
 
     def coulomb(self, NC, v, n_vb, n_cb, coulomb_region_type=0):
         """coulomb_matrix_elements for the states v (N_H x (2 n_vb + 2 n_cb), VB

@@ -131,7 +131,7 @@ def test_molecule_15_window_64(molecule, prec):
         assert dproj.max() < 1e-6
         assert dbloch < 1e-9
         assert res.max() < 1e-9 * max(hn, 1.0)
-        assert orth < 1e-12
+        assert orth < 1e-11
     else:
         assert dE.max() < 1e-6
         assert dproj.max() < 1e-3

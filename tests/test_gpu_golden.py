@@ -1,12 +1,22 @@
 """The CUDA path end to end on the reference's own example (GPU): Prism_111
-energies and Bloch characters against PWEM_test_ref/energies_*.dat."""
+(N_H = 10648) against PWEM_test_ref:
+* energies and Bloch characters (energies_*.dat);
+* momentum matrix elements: sums of |p|^2 over CB pair x VB pair blocks for
+  the five polarisations of momentum_matrix_elements.dat;
+* probability densities of the [100], [001] and [111] line scans, summed over
+  each Kramers pair (probability_density_*.dat).
+The fixtures are extracted by tests/golden/make_golden.py."""
 
 import os
+
+import json
 
 import numpy as np
 import pytest
 
 import qudos_b200 as q
+from oracle import envelope
+from test_oracle_golden import momentum_pair_sums, probability_pairs
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "prism_111")
@@ -30,3 +40,26 @@ def test_prism_111_golden(prec):
     tol = 1e-6 if prec == q.QD_PREC_FP64 else 1e-3
     assert np.abs(_kramers(vb) - _kramers(gvb)).max() < tol
     assert np.abs(_kramers(cb) - _kramers(gcb)).max() < tol
+
+
+@pytest.mark.parametrize("prec", [q.QD_PREC_FP64, q.QD_PREC_MIXED])
+def test_prism_111_momentum_and_densities_golden(prec):
+    pr = q.Problem(GOLDEN)
+    w, v = pr.solve(prec)
+    nv, nc = 2 * pr.n_vb, 2 * pr.n_cb
+    tol = 1e-8 if prec == q.QD_PREC_FP64 else 1e-4
+    gold = json.load(open(os.path.join(GOLDEN, "momentum_pairs.json")))
+    ours = momentum_pair_sums(pr.momentum(v, nv, nc))
+    ref = np.array(gold["pair_sums"])
+    assert np.abs(ours - ref).max() <= tol * np.abs(ref).max()
+    dens = np.load(os.path.join(GOLDEN, "probability_pairs.npz"))
+    geo = pr.geometry(pr.n_shape)[0]
+    L = (geo["L1"], geo["L2"], geo["L3"])
+    ptol = 1e-5 if prec == q.QD_PREC_FP64 else 1e-4
+    for d, tag in ((0, "100"), (2, "001"), (6, "111")):
+        x, y, z = envelope.linescan_grid(d, 300, L)
+        P = pr.envelopes(v, x, y, z)[1]
+        vb = probability_pairs(P, [nv - 1 - k for k in range(nv)])
+        cb = probability_pairs(P, [nv + k for k in range(nc)])
+        for o, r in ((vb, dens["vb_" + tag]), (cb, dens["cb_" + tag])):
+            assert np.all(np.abs(o - r) <= ptol * np.abs(r).max() + 2e-6 * np.abs(r)), tag
