@@ -374,11 +374,6 @@ int qd_tc_xprod(const void *A, int64_t lda, int64_t n, int64_t off, int m, const
 int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void *V, const void *W, int64_t ldv, int64_t voff,
                 int K, QdTcWork *w, void *stream);
 
-/* Issuer layout of the X-product kernel: 2 (default) two MMA-issuing warps
- * with 128 x 64 MMAs, 1 one issuer with 128 x 128 MMAs over [B_hi; B_lo].
- * Both compute the same product; QD_XPROD_ISSUERS sets the default. */
-int qd_tc_set_xprod_issuers(int issuers);
-
 /* Per-kernel device time of the tensor-core building blocks since the last
  * call (CUDA events around every launch, on the launching stream): which 0
  * is the X product (work = bytes of the trailing matrix read, 8 m^2 per

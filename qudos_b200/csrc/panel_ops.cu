@@ -133,25 +133,27 @@ template <typename R, int KU>
 __global__ void __launch_bounds__(256) tsmm_cn_kernel(int m, const cpx<R> *__restrict__ A, int64_t lda, int k1,
                                                       const cpx<R> *__restrict__ B, int64_t ldb, int nc,
                                                       int rows_per_slice, cpx<R> *__restrict__ part) {
+    // rows padded by one element so that the row-wise (coalesced) global loads
+    // of a warp land in distinct banks
+    constexpr int KW = 32 * KU + 1, BW = 33;
     extern __shared__ unsigned char cn_smem[];
-    cpx<R> *As = (cpx<R> *)cn_smem;     // [CN_RC][32 KU]
-    cpx<R> *Bs = As + CN_RC * 32 * KU;  // [CN_RC][32]
+    cpx<R> *As = (cpx<R> *)cn_smem;  // [CN_RC][KW]
+    cpx<R> *Bs = As + CN_RC * KW;    // [CN_RC][BW]
     const int ti = threadIdx.x & 31, tj = threadIdx.x >> 5;
     const int r0 = blockIdx.x * rows_per_slice, r1 = min(m, r0 + rows_per_slice);
-    constexpr int KW = 32 * KU;
     cpx<R> acc[KU][4];
 #pragma unroll
     for (int u = 0; u < KU; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) acc[u][v] = mk<R>(0, 0);
     for (int rb = r0; rb < r1; rb += CN_RC) {
-        for (int e = threadIdx.x; e < CN_RC * KW; e += 256) {
+        for (int e = threadIdx.x; e < CN_RC * 32 * KU; e += 256) {
             const int r = e % CN_RC, i = e / CN_RC;
             As[r * KW + i] = (rb + r < r1 && i < k1) ? A[(rb + r) + (int64_t)i * lda] : mk<R>(0, 0);
         }
         for (int e = threadIdx.x; e < CN_RC * 32; e += 256) {
             const int r = e % CN_RC, j = e / CN_RC;
-            Bs[r * 32 + j] = (rb + r < r1 && j < nc) ? B[(rb + r) + (int64_t)j * ldb] : mk<R>(0, 0);
+            Bs[r * BW + j] = (rb + r < r1 && j < nc) ? B[(rb + r) + (int64_t)j * ldb] : mk<R>(0, 0);
         }
         __syncthreads();
 #pragma unroll 2
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(256) tsmm_cn_kernel(int m, const cpx<R> *__res
 #pragma unroll
             for (int u = 0; u < KU; u++) a[u] = cconj(As[r * KW + ti + 32 * u]);
 #pragma unroll
-            for (int v = 0; v < 4; v++) b[v] = Bs[r * 32 + 4 * tj + v];
+            for (int v = 0; v < 4; v++) b[v] = Bs[r * BW + 4 * tj + v];
 #pragma unroll
             for (int u = 0; u < KU; u++)
 #pragma unroll
@@ -181,19 +183,25 @@ __global__ void __launch_bounds__(256) tsmm_cn_kernel(int m, const cpx<R> *__res
     }
 }
 
-// C[i + j ldc] = sum over slices of part[s][j k1 + i], in FP64, in slice order.
+// C[i + j ldc] = sum over slices of part[s][j k1 + i] in FP64: one warp per
+// output, lane l adds the slices l, l + 32, ..., then a fixed shuffle tree
+// (the same order on every run).
 template <typename R>
-__global__ void cn_reduce_kernel(const cpx<R> *__restrict__ part, int slices, int k1, int nc, cpx<R> *C, int64_t ldc) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) cn_reduce_kernel(const cpx<R> *__restrict__ part, int slices, int k1, int nc,
+                                                        cpx<R> *C, int64_t ldc) {
+    const int o = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (o >= k1 * nc) return;
     double sr = 0.0, si = 0.0;
-    for (int s = 0; s < slices; s++) {
+    for (int s = lane; s < slices; s += 32) {
         const cpx<R> v = part[(int64_t)s * k1 * nc + o];
         sr += (double)v.re;
         si += (double)v.im;
     }
-    const int i = o % k1, j = o / k1;
-    C[i + (int64_t)j * ldc] = mk<R>((R)sr, (R)si);
+    for (int d = 16; d > 0; d >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, d);
+        si += __shfl_xor_sync(0xffffffffu, si, d);
+    }
+    if (lane == 0) C[(o % k1) + (int64_t)(o / k1) * ldc] = mk<R>((R)sr, (R)si);
 }
 
 // C[n1 x n2] = alpha A[k x n1]^H B[k x n2], small (one CTA, FP64 sums).
@@ -223,9 +231,10 @@ int nsm() {
     return g_nsm;
 }
 
-// Rows per slice and slice count of tsmm_cn for m rows.
+// Rows per slice and slice count of tsmm_cn for m rows: one wave of at most
+// one CTA per SM, at least 64 rows each.
 void cn_slices(int m, int *rows, int *slices) {
-    int s = 2 * nsm();
+    int s = nsm();
     int r = (m + s - 1) / s;
     if (r < 64) r = 64;
     r = ((r + CN_RC - 1) / CN_RC) * CN_RC;
@@ -250,7 +259,7 @@ int cn_launch(int slices, size_t smem, cudaStream_t st, int m, const cpx<R> *A, 
     static int cfg = 0;
     if (!cfg) {
         CUDA_OK(cudaFuncSetAttribute(tsmm_cn_kernel<R, KU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(cpx<R>) * CN_RC * (32 * KU + 32))));
+                                     (int)(sizeof(cpx<R>) * CN_RC * (32 * KU + 1 + 33))));
         cfg = 1;
     }
     tsmm_cn_kernel<R, KU><<<slices, 256, smem, st>>>(m, A, lda, k1, B, ldb, nc, rows, scratch);
@@ -270,7 +279,7 @@ int tsmm_cn(int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B, int64_
     int rows, slices;
     cn_slices(m, &rows, &slices);
     const int ku = (k1 + 31) / 32;
-    const size_t smem = sizeof(cpx<R>) * (size_t)CN_RC * (32 * ku + 32);
+    const size_t smem = sizeof(cpx<R>) * (size_t)CN_RC * (32 * ku + 1 + 33);
     qd_count_launch(2);
     int rc = QD_OK;
     switch (ku) {
@@ -285,7 +294,7 @@ int tsmm_cn(int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B, int64_
     }
     if (rc) return rc;
     const int nout = k1 * nc;
-    cn_reduce_kernel<R><<<(nout + 255) / 256, 256, 0, st>>>(scratch, slices, k1, nc, C, ldc);
+    cn_reduce_kernel<R><<<(nout + 7) / 8, 256, 0, st>>>(scratch, slices, k1, nc, C, ldc);
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }

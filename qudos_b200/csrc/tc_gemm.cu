@@ -331,12 +331,8 @@ constexpr int X_L_COL0 = 2 * X_ISSUERS * X_N;
 constexpr int X_TMEM_COLS = 512;
 static_assert(X_L_COL0 + 2 * BKF * XL_STAGES <= X_TMEM_COLS, "TMEM columns");
 
-// Epilogue of the X product: every accumulation chunk is the sum of two
-// 64-column accumulators of this warp's lane quarter.  With two issuers (ISS
-// = 2) they are the issuers' accumulators, at columns 64 (2 h + ab); with one
-// issuer (ISS = 1) the two halves of its 128-column accumulator at 128 ab
-// (hi*hi + lo*hi in the first half, hi*lo in the second).
-template <int ISS>
+// Epilogue of the X product: every accumulation chunk is the sum of the two
+// issuers' accumulators (columns 64 (2 h + ab) of this warp's lane quarter).
 __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t tmem_base, int q, int &ab,
                                            uint32_t &aphase, uint64_t *tfull, uint64_t *tempty,
                                            volatile int *abort_flag) {
@@ -348,8 +344,7 @@ __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t 
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             uint32_t v[X_N];
-            const uint32_t col = ISS == 2 ? (uint32_t)((h * 2 + ab) * X_N) : (uint32_t)(ab * 2 * X_N + h * X_N);
-            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + col;
+            const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((h * 2 + ab) * X_N);
             tmem_ld32_issue(ta, v);
             tmem_ld32_issue(ta + 32, v + 32);
             tmem_ld_wait();
@@ -367,15 +362,6 @@ __device__ __forceinline__ bool drain_pair(float (&acc)[X_N], int nch, uint32_t 
     return true;
 }
 
-// ISS = 2: two MMA-issuing warps (1 and 11), each with its own double-buffered
-// 64-column accumulator, K steps 2h and 2h + 1 of every k-block, three
-// 128 x 64 x 8 MMAs per K step (hi*hi, hi*lo, lo*hi).
-// ISS = 1: warp 1 alone issues every K step as two MMAs: 128 x 128 x 8 with B
-// = [B_hi; B_lo] (the two 64-row halves of the B stage are adjacent, so one
-// descriptor spans both: hi*hi and hi*lo at once) and 128 x 64 x 8 lo*hi into
-// the first half; eight MMAs per k-block instead of twelve, each A tile read
-// from tensor memory twice instead of three times.
-template <int ISS>
 __global__ void __launch_bounds__(X_WARPS * 32, 1)
     xprod_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmBlo, TcArgs args) {
@@ -402,13 +388,13 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         for (int s = 0; s < XB_STAGES; s++) mbar_init(&fullB[s], 1);
         for (int s = 0; s < XL_STAGES; s++) {
             mbar_init(&conv[s], 4);  // one arrival per converter warp
-            mbar_init(&emptyL[s], ISS);
+            mbar_init(&emptyL[s], X_ISSUERS);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&tfull[b], ISS);
+            mbar_init(&tfull[b], X_ISSUERS);
             mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
-        mbar_init(done, ISS);
+        mbar_init(done, X_ISSUERS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -468,9 +454,9 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
         }
     } else if (warp == 1 || warp == 11) {
         // ---------------- MMA issuers (accumulation restarted every X_CHUNK k-blocks) ----------------
-        if (lane == 0 && (ISS == 2 || warp == 1)) {
-            const int h = warp == 11;  // ISS = 2: K steps 2h, 2h + 1 of every k-block
-            const uint32_t idesc = tf32_idesc(TILE_M, X_N), idesc2 = tf32_idesc(TILE_M, 2 * X_N);
+        if (lane == 0) {
+            const int h = warp == 11;  // K steps 2h, 2h + 1 of every k-block
+            const uint32_t idesc = tf32_idesc(TILE_M, X_N);
             const uint64_t bdesc0 = sw128_desc(smem_u32(ringB));
             int sb = 0, sl = 0, ab = 0;
             uint32_t pb = 0, pl = 0, aphase = 0;
@@ -494,31 +480,18 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
                         break;
                     }
                     tc_fence_after();
-                    if (ISS == 2) {
-                        const uint32_t d = tmem_base + (uint32_t)((h * 2 + ab) * X_N);
-                        const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF + h * 16);
-                        const uint32_t a_lo = a_hi + BKF;
-                        // +32 bytes along K in the B tile = +2 in the descriptor's address field
-                        const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES + h * 64) >> 4);
-                        const uint64_t bl = bh + (X_B_BYTES >> 4);
+                    const uint32_t d = tmem_base + (uint32_t)((h * 2 + ab) * X_N);
+                    const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF + h * 16);
+                    const uint32_t a_lo = a_hi + BKF;
+                    // +32 bytes along K in the B tile = +2 in the descriptor's address field
+                    const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES + h * 64) >> 4);
+                    const uint64_t bl = bh + (X_B_BYTES >> 4);
 #pragma unroll
-                        for (int kk = 0; kk < 2; kk++) {
-                            uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
-                            umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc, acc);
-                            umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
-                            umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
-                        }
-                    } else {
-                        const uint32_t d = tmem_base + (uint32_t)(ab * 2 * X_N);
-                        const uint32_t a_hi = tmem_base + (uint32_t)(X_L_COL0 + sl * 2 * BKF);
-                        const uint32_t a_lo = a_hi + BKF;
-                        const uint64_t bh = bdesc0 + (uint64_t)((sb * 2 * X_B_BYTES) >> 4);
-#pragma unroll
-                        for (int kk = 0; kk < 4; kk++) {
-                            uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
-                            umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc2, acc);  // [hi*hi | hi*lo]
-                            umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);    // + lo*hi (first half)
-                        }
+                    for (int kk = 0; kk < 2; kk++) {
+                        uint32_t acc = (cpos > 0 || kk > 0) ? 1u : 0u;
+                        umma_tf32_ts(d, a_hi + kk * 8, bh + 2 * kk, idesc, acc);
+                        umma_tf32_ts(d, a_hi + kk * 8, bl + 2 * kk, idesc, 1u);
+                        umma_tf32_ts(d, a_lo + kk * 8, bh + 2 * kk, idesc, 1u);
                     }
                     umma_commit(&emptyL[sl]);  // frees B stage sb == sl and TMEM stage sl
                     ring_next(sb, pb, XB_STAGES);
@@ -544,7 +517,7 @@ __global__ void __launch_bounds__(X_WARPS * 32, 1)
             int tm, sp, kb0, kb1;
             xprod_item(args, item, tm, sp, kb0, kb1);
             float acc[X_N];
-            if (!drain_pair<ISS>(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, ab, aphase, tfull, tempty,
+            if (!drain_pair(acc, (kb1 - kb0 + X_CHUNK - 1) / X_CHUNK, tmem_base, q, ab, aphase, tfull, tempty,
                                  abort_flag)) {
                 fail(4);
                 break;
@@ -626,6 +599,9 @@ constexpr int F_A_BYTES = TILE_M * BKF * 4;  // 16 KB
 constexpr int F_B_BYTES = F_N * BKF * 4;     // 32 KB
 constexpr int F_STAGE_BYTES = 2 * F_A_BYTES + 2 * F_B_BYTES;
 constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES;
+// Epilogue staging for the mirrored (upper-triangle) stores: per epilogue
+// warp 8 columns x 32 rows of complex64 (one batch of F_LD columns).
+constexpr int F_MIRROR_BYTES = 8 * 8 * 33 * 8;
 constexpr int F_EPI_COLS = 128;
 #ifndef F_CHUNK
 #define F_CHUNK 2  // k-blocks per accumulation chunk
@@ -767,13 +743,19 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
                 break;
             }
             const int row = tm * TILE_M + r;
-            if (row >= args.rows) continue;
-            float2 *Crow = args.C + row;                            // C[row, :]
-            float2 *Ccol = args.C + (int64_t)row * args.ldc;        // C[:, row] (mirror)
+            const int row0 = tm * TILE_M + q * 32;  // first row of this warp
+            float2 *Crow = args.C + row;             // C[row, :]
             const int col0 = tn * (F_N / 2) + cbase / 2;
+            // this warp's staging area: stage[j][rr] = updated C[row0 + rr, col0 + j0 + j]
+            // (after the 512 bytes of barriers that follow the operand stages)
+            float2(*stage)[33] = (float2(*)[33])(smem + F_SMEM + 512 + (warp - 2) * (8 * 33 * 8));
             // Batches of F_LD columns: all loads of a batch are issued before its
             // stores (a store may alias a later load, so the compiler would
-            // otherwise keep every load behind the previous store).
+            // otherwise keep every load behind the previous store).  The lower
+            // element goes back in place (32 consecutive rows of one column per
+            // store); its conjugate, the upper element (col, row), is staged in
+            // shared memory and stored transposed, so that lanes write runs of 8
+            // consecutive rows of a column of C instead of 32 separate columns.
             constexpr int F_LD = 8;
 #pragma unroll
             for (int j0 = 0; j0 < F_EPI_COLS / 2; j0 += F_LD) {
@@ -781,24 +763,36 @@ __global__ void __launch_bounds__(F_WARPS * 32, 1)
 #pragma unroll
                 for (int j = 0; j < F_LD; j++) {
                     const int col = col0 + j0 + j;
-                    cv[j] = (col < args.cols && col <= row) ? __ldcg(Crow + (int64_t)col * args.ldc)
-                                                            : make_float2(0.f, 0.f);
+                    cv[j] = (row < args.rows && col < args.cols && col <= row) ? __ldcg(Crow + (int64_t)col * args.ldc)
+                                                                              : make_float2(0.f, 0.f);
                 }
 #pragma unroll
                 for (int j = 0; j < F_LD; j++) {
                     const int col = col0 + j0 + j;
-                    if (col >= args.cols || col > row) continue;
                     float2 c = cv[j];
                     c.x -= acc[2 * (j0 + j)];
                     c.y -= acc[2 * (j0 + j) + 1];
-                    if (col == row) {
-                        c.y = 0.f;
-                        Crow[(int64_t)col * args.ldc] = c;
-                    } else {
-                        Crow[(int64_t)col * args.ldc] = c;
-                        Ccol[col] = make_float2(c.x, -c.y);
+                    if (col == row) c.y = 0.f;
+                    if (row < args.rows && col < args.cols && col <= row) Crow[(int64_t)col * args.ldc] = c;
+                    stage[j][lane] = c;
+                }
+                __syncwarp();
+                // mirror: lane (rr, cc) stores rows row0 + rr + 4 it of column col0 + j0 + cc of the
+                // tile's transpose, i.e. C[col0 + j0 + cc, row0 + rr + 4 it] = conj(stage[cc][rr + 4 it])
+                {
+                    const int cc = lane & 7, rr = lane >> 3;
+                    const int mcol = col0 + j0 + cc;  // row index of the upper element
+#pragma unroll
+                    for (int it = 0; it < 8; it++) {
+                        const int rl = rr + 4 * it;
+                        const int mrow = row0 + rl;  // column index of the upper element
+                        if (mrow < args.rows && mcol < args.cols && mcol < mrow) {
+                            const float2 v = stage[cc][rl];
+                            args.C[mcol + (int64_t)mrow * args.ldc] = make_float2(v.x, -v.y);
+                        }
                     }
                 }
+                __syncwarp();
             }
         }
     }
@@ -960,35 +954,19 @@ void timer_mark(int which, cudaStream_t st) {
     cudaEventRecord(t.ev[t.used++], st);
 }
 
-// Issuer layout of the X product: 1 selects the single issuer with
-// 128-column MMAs, 2 the two issuers (QD_XPROD_ISSUERS in the environment, or
-// qd_tc_set_xprod_issuers).
-int g_xprod_issuers = -1;
-int xprod_issuers() {
-    if (g_xprod_issuers < 0) {
-        const char *e = getenv("QD_XPROD_ISSUERS");
-        g_xprod_issuers = (e && atoi(e) == 1) ? 1 : 2;
-    }
-    return g_xprod_issuers;
-}
-
 int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &blo, const TcArgs &args,
                  cudaStream_t st) {
     static bool configured = false;
     const int smem = X_SMEM + SMEM_EXTRA;
     if (!configured) {
-        CUDA_OK(cudaFuncSetAttribute(xprod_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        CUDA_OK(cudaFuncSetAttribute(xprod_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_OK(cudaFuncSetAttribute(xprod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         configured = true;
     }
     int grid = args.n_items < sm_count() ? args.n_items : sm_count();
     if (grid < 1) return QD_OK;
     qd_count_launch(1);
     timer_mark(0, st);
-    if (xprod_issuers() == 1)
-        xprod_kernel<1><<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
-    else
-        xprod_kernel<2><<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
+    xprod_kernel<<<grid, X_WARPS * 32, smem, st>>>(a, b, blo, args);
     CUDA_OK(cudaGetLastError());
     timer_mark(0, st);
     g_timer[0].work += 8.0 * (double)args.rows * (double)args.rows;
@@ -998,7 +976,7 @@ int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &
 int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap &b, const CUtensorMap &blo,
                  const TcArgs &args, cudaStream_t st) {
     static bool configured = false;
-    const int smem = F_SMEM + SMEM_EXTRA;
+    const int smem = F_SMEM + F_MIRROR_BYTES + SMEM_EXTRA;
     if (!configured) {
         CUDA_OK(cudaFuncSetAttribute(flush_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         configured = true;
@@ -1015,12 +993,6 @@ int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap
 }
 
 }  // namespace
-
-extern "C" int qd_tc_set_xprod_issuers(int issuers) {
-    if (issuers != 1 && issuers != 2) return qd_set_error(QD_ERR_ARG, "X product issuers must be 1 or 2");
-    g_xprod_issuers = issuers;
-    return QD_OK;
-}
 
 // Limit of the pipeline waits for the current device (ns; negative: default).
 extern "C" int qd_tc_set_wait_limit(long long ns) {

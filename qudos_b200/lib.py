@@ -110,7 +110,6 @@ _sig("qd_tc_work_free", None, [vp])
 _sig("qd_tc_work_check", ci, [vp])
 _sig("qd_tc_xprod", ci, [vp, i64, i64, i64, ci, vp, i64, ci, vp, i64, vp, vp])
 _sig("qd_tc_flush", ci, [vp, i64, i64, ci, vp, vp, i64, i64, ci, vp, vp])
-_sig("qd_tc_set_xprod_issuers", ci, [ci])
 _sig("qd_tc_kernel_stats", ci, [ci, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)])
 _sig("qd_gemm_peak", ci, [ci, ci, ci, C.POINTER(C.c_double)])
 _sig("qd_tsmm_nn", ci, [ci, ci, ci, ci, C.POINTER(vp), C.POINTER(i64), C.POINTER(vp), C.POINTER(i64), C.POINTER(ci),
@@ -151,8 +150,8 @@ class Complex128(C.Structure):
     _fields_ = [("re", C.c_double), ("im", C.c_double)]
 
 
-_sig("hamiltonian_derivative_8_band", None, [ci, WaveVectors, C.POINTER(SupercellGeometry), C.POINTER(MaterialParams),
-                                             vp])
+_sig("hamiltonian_derivative_8_band", None, [ci, ci, WaveVectors, C.POINTER(SupercellGeometry),
+                                             C.POINTER(MaterialParams), vp])
 _sig("momentum_matrix_element", Complex128, [ci, ci, WaveVectors, C.POINTER(SupercellGeometry),
                                              C.POINTER(MaterialParams), Eigenstate, C.c_int64, Eigenstate, C.c_int64,
                                              C.POINTER(ci)])

@@ -81,9 +81,16 @@ class ReferenceCall:
         shp = (2 * N - 1,) * 3
         pr.build_tables()
         chi = [None] + [pr.table(0, s, 0, shp) for s in range(1, ns)]
-        eps = [pr.table(1, c, 0, shp) for c in range(6)]
-        phi = pr.table(2, 0, 0, shp)
-        conv = [None] + [[pr.table(3, s, c, shp) for c in range(8)] for s in range(1, ns)]
+
+        def optional(fn):  # tables of a disabled stage (no strain, no piezo) do not exist
+            try:
+                return fn()
+            except L.QDError:
+                return None
+
+        eps = optional(lambda: [pr.table(1, c, 0, shp) for c in range(6)])
+        phi = optional(lambda: pr.table(2, 0, 0, shp)) if eps is not None else None
+        conv = optional(lambda: [None] + [[pr.table(3, s, c, shp) for c in range(8)] for s in range(1, ns)])
         F, K = pr.field()
         return cls((N, N, N), geo, mat, chi, eps, conv, phi, F=F, K=K)
 

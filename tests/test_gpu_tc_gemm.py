@@ -49,10 +49,9 @@ def need_gpu():
     assert q.device_count() > 0, "no CUDA device visible"
 
 
-@pytest.mark.parametrize("issuers", [2, 1])
 @pytest.mark.parametrize("n,off,nb", [(512, 0, 32), (1000, 64, 32), (1000, 64, 17), (2048, 990, 32), (336, 328, 8),
                                       (6144, 32, 32)])
-def test_xprod(n, off, nb, issuers):
+def test_xprod(n, off, nb):
     rng = np.random.default_rng(n + off + nb)
     A = _hermitian(rng, n)
     m = n - off
@@ -60,14 +59,10 @@ def test_xprod(n, off, nb, issuers):
     w = _Work(n, 256)
     dA, dV = _dev(A), _dev(VT)
     dX = L.DeviceBuffer(m * 32 * 8)
-    L.check(L.lib.qd_tc_set_xprod_issuers(issuers))
-    try:
-        for _ in range(2):  # second call reuses the work buffers
-            L.check(L.lib.qd_tc_xprod(dA.ptr, n, n, off, m, dV.ptr, m, nb, dX.ptr, m, w.p, None))
-            L.check(L.lib.qd_device_synchronize())
-            L.check(L.lib.qd_tc_work_check(w.p))
-    finally:
-        L.check(L.lib.qd_tc_set_xprod_issuers(2))
+    for _ in range(2):  # second call reuses the work buffers
+        L.check(L.lib.qd_tc_xprod(dA.ptr, n, n, off, m, dV.ptr, m, nb, dX.ptr, m, w.p, None))
+        L.check(L.lib.qd_device_synchronize())
+        L.check(L.lib.qd_tc_work_check(w.p))
     X = dX.download(np.empty((m, 32), dtype=np.complex64, order="F"))[:, :nb]
     A22 = A[off:, off:].astype(np.complex128)
     ref = A22 @ VT.astype(np.complex128)
