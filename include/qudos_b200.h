@@ -406,18 +406,19 @@ int qd_residual_norms_dev(int64_t n, const void *R, int64_t ldr, const void *Z, 
 /* Tall-and-skinny products of the panel steps (device pointers, column-major;
  * fp32 != 0 selects complex64, else complex128):
  *   qd_tsmm_nn  C[m x nc] = beta C + sum_t alpha[t] A[t] op(B[t]), nterms 1 or
- *               2, nc <= 32; op(B) = B (K x nc, ldb) when btrans[t] == 0, else
+ *               2, nc <= 64; op(B) = B (K x nc, ldb) when btrans[t] == 0, else
  *               B^H of an nc x K block;
- *   qd_tsmm_cn  C[k1 x nc] = A^H B reduced over m rows, k1 <= 256, nc <= 32;
- *               scratch holds qd_tsmm_cn_scratch_bytes(m, k1, nc, 8 or 16)
- *               bytes of partial sums, which are added in FP64 in a fixed
- *               order;
+ *   qd_tsmm_cn  C[k1 x nc] = A^H B reduced over m rows, k1 <= 256 with
+ *               nc <= 32 or k1 <= 64 with nc <= 64; scratch holds
+ *               scratch_bytes >= qd_tsmm_cn_scratch_bytes(m, k1, nc, 8 or 16)
+ *               of partial sums (QD_ERR_ARG when too small), which are
+ *               added in FP64 in a fixed order;
  *   qd_small_cn C[n1 x n2] = alpha A^H B for small k x n1, k x n2 inputs. */
 int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const *A, const int64_t *lda, const void *const *B,
                const int64_t *ldb, const int *K, const int *btrans, const double *alpha, void *C, int64_t ldc,
                double beta, void *stream);
 int qd_tsmm_cn(int fp32, int m, const void *A, int64_t lda, int k1, const void *B, int64_t ldb, int nc, void *C,
-               int64_t ldc, void *scratch, void *stream);
+               int64_t ldc, void *scratch, size_t scratch_bytes, void *stream);
 int qd_small_cn(int fp32, int k, int n1, int n2, const void *A, int lda, const void *B, int ldb, double alpha,
                 void *C, int ldc, void *stream);
 size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes);

@@ -13,6 +13,7 @@ struct cpx {
 struct Stage1Work {
     void *VT, *X, *M, *Y, *Tall, *Rall, *Vacc, *Wacc, *S1, *S2, *gram, *tau;
     void *part;  // partial sums of the tall A^H B reductions (panel_ops.cu)
+    size_t part_bytes;
     struct QdTcWork *tc;  // tensor-core GEMM work buffers (mixed path), or null
     double2 *red, *rowbuf;
     unsigned *bar;

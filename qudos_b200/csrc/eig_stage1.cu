@@ -330,13 +330,13 @@ extern "C" int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const
                           const void *const *B, const int64_t *ldb, const int *K, const int *btrans,
                           const double *alpha, void *C, int64_t ldc, double beta, void *stream);
 extern "C" int qd_tsmm_cn(int fp32, int m, const void *A, int64_t lda, int k1, const void *B, int64_t ldb, int nc,
-                          void *C, int64_t ldc, void *scratch, void *stream);
+                          void *C, int64_t ldc, void *scratch, size_t scratch_bytes, void *stream);
 extern "C" int qd_small_cn(int fp32, int k, int n1, int n2, const void *A, int lda, const void *B, int ldb,
                            double alpha, void *C, int ldc, void *stream);
 extern "C" size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes);
 
 // One- or two-term tall product C[m x nc] = beta C + sum alpha_t A_t op(B_t),
-// 32 output columns per launch.
+// up to 64 output columns per launch.
 template <typename T>
 static int nn(cudaStream_t st, int m, int nc, const T *A0, int64_t lda0, const T *B0, int64_t ldb0, int K0, int bt0,
               double al0, T *C, int64_t ldc, double beta, const T *A1 = nullptr, int64_t lda1 = 0,
@@ -346,8 +346,8 @@ static int nn(cudaStream_t st, int m, int nc, const T *A0, int64_t lda0, const T
     int K[2] = {K0, K1}, bt[2] = {bt0, bt1};
     double al[2] = {al0, al1};
     const int fp32 = sizeof(T) == 8;
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-        const int w = nc - c0 < 32 ? nc - c0 : 32;
+    for (int c0 = 0; c0 < nc; c0 += 64) {
+        const int w = nc - c0 < 64 ? nc - c0 : 64;
         const void *Bc[2];
         for (int t = 0; t < 2; t++)
             Bc[t] = B[t] ? (const void *)((const T *)B[t] + (bt[t] ? c0 : c0 * lb[t])) : nullptr;
@@ -356,14 +356,16 @@ static int nn(cudaStream_t st, int m, int nc, const T *A0, int64_t lda0, const T
     }
     return QD_OK;
 }
-// C[k1 x nc] = A[m x k1]^H B[m x nc] (k1 <= 256), 32 output columns per launch.
+// C[k1 x nc] = A[m x k1]^H B[m x nc] (k1 <= 256): 64 output columns per launch
+// when k1 <= 64, else 32.  part holds part_bytes of partial sums.
 template <typename T>
 static int cn(cudaStream_t st, int m, const T *A, int64_t lda, int k1, const T *B, int64_t ldb, int nc, T *C,
-              int64_t ldc, void *part) {
+              int64_t ldc, void *part, size_t part_bytes) {
     const int fp32 = sizeof(T) == 8;
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-        const int w = nc - c0 < 32 ? nc - c0 : 32;
-        int rc = qd_tsmm_cn(fp32, m, A, lda, k1, B + c0 * ldb, ldb, w, C + c0 * ldc, ldc, part, st);
+    const int cw = k1 <= 64 ? 64 : 32;
+    for (int c0 = 0; c0 < nc; c0 += cw) {
+        const int w = nc - c0 < cw ? nc - c0 : cw;
+        int rc = qd_tsmm_cn(fp32, m, A, lda, k1, B + c0 * ldb, ldb, w, C + c0 * ldc, ldc, part, part_bytes, st);
         if (rc) return rc;
     }
     return QD_OK;
@@ -530,7 +532,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         RC(launch_panel<T>(P, lda, m, b, nb, Rp, (T *)w.tau, w, st));
         // 3. T from the Gram matrix
         prof_mark(2, st);
-        RC(cn<T>(st, m, P, lda, nb, P, lda, nb, (T *)w.gram, b, w.part));
+        RC(cn<T>(st, m, P, lda, nb, P, lda, nb, (T *)w.gram, b, w.part, w.part_bytes));
         qd_count_launch(1);
         {
             static int ft_configured[2] = {0, 0};
@@ -562,14 +564,14 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
         prof_mark(4, st);
         if (K > 0) {
             T *S1 = (T *)w.S1, *S2 = (T *)w.S2;
-            RC(cn<T>(st, m, Wacc + off + b, ldv, K, VT, m, nb, S1, w.agg, w.part));
-            RC(cn<T>(st, m, Vacc + off + b, ldv, K, VT, m, nb, S2, w.agg, w.part));
+            RC(cn<T>(st, m, Wacc + off + b, ldv, K, VT, m, nb, S1, w.agg, w.part, w.part_bytes));
+            RC(cn<T>(st, m, Vacc + off + b, ldv, K, VT, m, nb, S2, w.agg, w.part, w.part_bytes));
             RC(nn<T>(st, m, nb, Vacc + off + b, ldv, S1, w.agg, K, 0, -1.0, X, ldv, 1.0, Wacc + off + b, ldv, S2,
                      w.agg, K, 0, -1.0));
         }
         // 6. W = X - 1/2 V (T^H V^H X)
         prof_mark(5, st);
-        RC(cn<T>(st, m, P, lda, nb, X, ldv, nb, (T *)w.M, b, w.part));
+        RC(cn<T>(st, m, P, lda, nb, X, ldv, nb, (T *)w.M, b, w.part, w.part_bytes));
         RC(qd_small_cn(sizeof(T) == 8, nb, nb, nb, Tp, b, w.M, b, 1.0, w.Y, b, st));
         RC(nn<T>(st, m, nb, P, lda, (T *)w.Y, b, nb, 0, -0.5, X, ldv, 1.0));
         // 7. append V (zero above its first row) to Vacc; W already sits in Wacc
@@ -622,6 +624,7 @@ extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, 
     size_t sizes[] = {eb * n * b, eb * 16, eb * b * b, eb * b * b, eb * (size_t)(w->npanels + 1) * b * b,
                       eb * (size_t)(w->npanels + 1) * b * b, eb * n * agg, eb * n * agg, eb * agg * b,
                       eb * agg * b, eb * b * b, eb * b, qd_tsmm_cn_scratch_bytes((int)n, agg, 32, (int)eb)};
+    w->part_bytes = sizes[12];
     for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); i++)
         if (qd_pool_alloc(bufs[i], sizes[i], st) != 0) return qd_set_error(QD_ERR_NOMEM, "stage-1 workspace");
     int dev, nsm;
@@ -718,7 +721,7 @@ static int backtransform(const T *A, int64_t n, int64_t lda, int b, const Stage1
         const T *Tm = (const T *)w->Tall + (int64_t)p * b * b;
         T *Zs = Z + (k + b);
         T *M = (T *)w->VT, *Y = (T *)w->Vacc;
-        RC(cn<T>(st, m, V, lda, nb, Zs, ldz, mz, M, nb, w->part));     // M = V^H Z
+        RC(cn<T>(st, m, V, lda, nb, Zs, ldz, mz, M, nb, w->part, w->part_bytes));     // M = V^H Z
         RC(nn<T>(st, nb, mz, Tm, b, M, nb, nb, 0, 1.0, Y, nb, 0.0));    // Y = T M
         RC(nn<T>(st, m, mz, V, lda, Y, nb, nb, 0, -1.0, Zs, ldz, 1.0));  // Z -= V Y
     }

@@ -4,13 +4,15 @@
 // (the m rows of the trailing matrix) and short others (the b = 32 panel
 // columns and the K <= 256 pending reflector columns):
 //
-//   tsmm_nn  C[m x nc] = beta C + sum_t alpha_t A_t[m x K_t] op(B_t)[K_t x nc]
+//   tsmm_nn  C[m x nc] = beta C + sum_t alpha_t A_t[m x K_t] op(B_t)[K_t x nc],
+//            nc <= 64
 //            (up to two terms; op(B) is B or B^H of an nc x K block).  One CTA
 //            per 128-row tile; the K dimension is streamed through shared
 //            memory in chunks of 16.  Serves the panel refresh
 //            (P -= V Wb^H + W Vb^H), V T, the corrections (X -= V S1 + W S2),
 //            W = X - 1/2 V Y and the back-transformation (Z -= V Y).
-//   tsmm_cn  C[k1 x nc] = A[m x k1]^H B[m x nc], k1 <= 256, nc <= 32: the rows
+//   tsmm_cn  C[k1 x nc] = A[m x k1]^H B[m x nc], k1 <= 256 with nc <= 32, or
+//            k1 <= 64 with nc <= 64: the rows
 //            are split into slices, each CTA accumulates its slice in the
 //            working precision, writes the partial, and a second kernel sums
 //            the partials in FP64 (a fixed order, so results do not depend on
@@ -52,21 +54,24 @@ __device__ __forceinline__ cpx<R> cfma_(cpx<R> acc, cpx<R> a, cpx<R> b) {
     return acc;
 }
 
-constexpr int NN_TM = 128, NN_KC = 16, NN_NC = 32;
+constexpr int NN_TM = 128;
 
-// Thread (tx, ty): rows tx + 32 i (i < 4), columns 4 ty + j (j < 4).
-template <typename R>
+// Thread (tx, ty): rows tx + 32 i (i < 4), columns NJ ty + j (j < NJ), NJ =
+// NCW / 8 for an output width of NCW = 32 or 64 columns.
+template <typename R, int NCW>
 __global__ void __launch_bounds__(256) tsmm_nn_kernel(int m, int nc, TsTerm<R> t0, TsTerm<R> t1, int nterms,
                                                       cpx<R> *C, int64_t ldc, R beta) {
+    // K chunk of 16 (8 for complex128 at 64 columns, to stay within 48 KB of static shared memory)
+    constexpr int NN_NC = NCW, NJ = NCW / 8, NN_KC = (sizeof(R) == 8 && NCW == 64) ? 8 : 16;
     __shared__ cpx<R> As[NN_KC][NN_TM];
-    __shared__ cpx<R> Bs[NN_KC][NN_NC];
+    __shared__ cpx<R> Bs[NN_KC][NN_NC + 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int r0 = blockIdx.x * NN_TM;
-    cpx<R> acc[4][4];
+    cpx<R> acc[4][NJ];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = mk<R>(0, 0);
+        for (int j = 0; j < NJ; j++) acc[i][j] = mk<R>(0, 0);
     for (int t = 0; t < nterms; t++) {
         const TsTerm<R> &T = t == 0 ? t0 : t1;
         for (int p0 = 0; p0 < T.K; p0 += NN_KC) {
@@ -92,15 +97,15 @@ __global__ void __launch_bounds__(256) tsmm_nn_kernel(int m, int nc, TsTerm<R> t
             __syncthreads();
 #pragma unroll 4
             for (int p = 0; p < NN_KC; p++) {
-                cpx<R> a[4], b[4];
+                cpx<R> a[4], b[NJ];
 #pragma unroll
                 for (int i = 0; i < 4; i++) a[i] = As[p][tx + 32 * i];
 #pragma unroll
-                for (int j = 0; j < 4; j++) b[j] = Bs[p][4 * ty + j];
+                for (int j = 0; j < NJ; j++) b[j] = Bs[p][NJ * ty + j];
 #pragma unroll
                 for (int i = 0; i < 4; i++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) acc[i][j] = cfma_(acc[i][j], a[i], b[j]);
+                    for (int j = 0; j < NJ; j++) acc[i][j] = cfma_(acc[i][j], a[i], b[j]);
             }
             __syncthreads();
         }
@@ -110,8 +115,8 @@ __global__ void __launch_bounds__(256) tsmm_nn_kernel(int m, int nc, TsTerm<R> t
         const int gr = r0 + tx + 32 * i;
         if (gr >= m) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int c = 4 * ty + j;
+        for (int j = 0; j < NJ; j++) {
+            const int c = NJ * ty + j;
             if (c >= nc) continue;
             cpx<R> *p = C + gr + (int64_t)c * ldc;
             cpx<R> v = acc[i][j];
@@ -128,45 +133,46 @@ __global__ void __launch_bounds__(256) tsmm_nn_kernel(int m, int nc, TsTerm<R> t
 constexpr int CN_RC = 32;  // rows per shared-memory chunk
 
 // Partial A^H B over one slice of rows.  Thread (ti, tj): outputs i = ti + 32 u
-// (u < KU), j = 4 tj + v (v < 4).  Partials: part[slice][j * k1 + i].
-template <typename R, int KU>
+// (u < KU), j = NV tj + v (v < NV), NV = NCW / 8 for NCW = 32 or 64 output
+// columns.  Partials: part[slice][j * k1 + i].
+template <typename R, int KU, int NCW>
 __global__ void __launch_bounds__(256) tsmm_cn_kernel(int m, const cpx<R> *__restrict__ A, int64_t lda, int k1,
                                                       const cpx<R> *__restrict__ B, int64_t ldb, int nc,
                                                       int rows_per_slice, cpx<R> *__restrict__ part) {
     // rows padded by one element so that the row-wise (coalesced) global loads
     // of a warp land in distinct banks
-    constexpr int KW = 32 * KU + 1, BW = 33;
+    constexpr int KW = 32 * KU + 1, BW = NCW + 1, NV = NCW / 8;
     extern __shared__ unsigned char cn_smem[];
     cpx<R> *As = (cpx<R> *)cn_smem;  // [CN_RC][KW]
     cpx<R> *Bs = As + CN_RC * KW;    // [CN_RC][BW]
     const int ti = threadIdx.x & 31, tj = threadIdx.x >> 5;
     const int r0 = blockIdx.x * rows_per_slice, r1 = min(m, r0 + rows_per_slice);
-    cpx<R> acc[KU][4];
+    cpx<R> acc[KU][NV];
 #pragma unroll
     for (int u = 0; u < KU; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[u][v] = mk<R>(0, 0);
+        for (int v = 0; v < NV; v++) acc[u][v] = mk<R>(0, 0);
     for (int rb = r0; rb < r1; rb += CN_RC) {
         for (int e = threadIdx.x; e < CN_RC * 32 * KU; e += 256) {
             const int r = e % CN_RC, i = e / CN_RC;
             As[r * KW + i] = (rb + r < r1 && i < k1) ? A[(rb + r) + (int64_t)i * lda] : mk<R>(0, 0);
         }
-        for (int e = threadIdx.x; e < CN_RC * 32; e += 256) {
+        for (int e = threadIdx.x; e < CN_RC * NCW; e += 256) {
             const int r = e % CN_RC, j = e / CN_RC;
             Bs[r * BW + j] = (rb + r < r1 && j < nc) ? B[(rb + r) + (int64_t)j * ldb] : mk<R>(0, 0);
         }
         __syncthreads();
 #pragma unroll 2
         for (int r = 0; r < CN_RC; r++) {
-            cpx<R> a[KU], b[4];
+            cpx<R> a[KU], b[NV];
 #pragma unroll
             for (int u = 0; u < KU; u++) a[u] = cconj(As[r * KW + ti + 32 * u]);
 #pragma unroll
-            for (int v = 0; v < 4; v++) b[v] = Bs[r * BW + 4 * tj + v];
+            for (int v = 0; v < NV; v++) b[v] = Bs[r * BW + NV * tj + v];
 #pragma unroll
             for (int u = 0; u < KU; u++)
 #pragma unroll
-                for (int v = 0; v < 4; v++) acc[u][v] = cfma_(acc[u][v], a[u], b[v]);
+                for (int v = 0; v < NV; v++) acc[u][v] = cfma_(acc[u][v], a[u], b[v]);
         }
         __syncthreads();
     }
@@ -176,8 +182,8 @@ __global__ void __launch_bounds__(256) tsmm_cn_kernel(int m, const cpx<R> *__res
         const int i = ti + 32 * u;
         if (i >= k1) continue;
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            const int j = 4 * tj + v;
+        for (int v = 0; v < NV; v++) {
+            const int j = NV * tj + v;
             if (j < nc) P[(int64_t)j * k1 + i] = acc[u][v];
         }
     }
@@ -245,52 +251,65 @@ void cn_slices(int m, int *rows, int *slices) {
 template <typename R>
 int tsmm_nn(int m, int nc, int nterms, const TsTerm<R> *terms, cpx<R> *C, int64_t ldc, R beta, cudaStream_t st) {
     if (m <= 0 || nc <= 0) return QD_OK;
-    if (nc > NN_NC) return qd_set_error(QD_ERR_ARG, "tsmm_nn: %d columns above %d", nc, NN_NC);
+    if (nc > 64) return qd_set_error(QD_ERR_ARG, "tsmm_nn: %d columns above 64", nc);
     TsTerm<R> t1 = nterms > 1 ? terms[1] : terms[0];
     qd_count_launch(1);
-    tsmm_nn_kernel<R><<<(unsigned)((m + NN_TM - 1) / NN_TM), 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta);
+    const unsigned grid = (unsigned)((m + NN_TM - 1) / NN_TM);
+    if (nc <= 32)
+        tsmm_nn_kernel<R, 32><<<grid, 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta);
+    else
+        tsmm_nn_kernel<R, 64><<<grid, 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta);
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }
 
-template <typename R, int KU>
-int cn_launch(int slices, size_t smem, cudaStream_t st, int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B,
+template <typename R, int KU, int NCW = 32>
+int cn_launch(int slices, cudaStream_t st, int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B,
               int64_t ldb, int nc, int rows, cpx<R> *scratch) {
+    const size_t smem = sizeof(cpx<R>) * (size_t)CN_RC * (32 * KU + 1 + NCW + 1);
     static int cfg = 0;
     if (!cfg) {
-        CUDA_OK(cudaFuncSetAttribute(tsmm_cn_kernel<R, KU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(cpx<R>) * CN_RC * (32 * KU + 1 + 33))));
+        CUDA_OK(cudaFuncSetAttribute(tsmm_cn_kernel<R, KU, NCW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
         cfg = 1;
     }
-    tsmm_cn_kernel<R, KU><<<slices, 256, smem, st>>>(m, A, lda, k1, B, ldb, nc, rows, scratch);
+    tsmm_cn_kernel<R, KU, NCW><<<slices, 256, smem, st>>>(m, A, lda, k1, B, ldb, nc, rows, scratch);
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }
 
 template <typename R>
 int tsmm_cn(int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B, int64_t ldb, int nc, cpx<R> *C,
-            int64_t ldc, cpx<R> *scratch, cudaStream_t st) {
+            int64_t ldc, cpx<R> *scratch, size_t scratch_bytes, cudaStream_t st) {
     if (k1 <= 0 || nc <= 0) return QD_OK;
-    if (k1 > 256 || nc > 32) return qd_set_error(QD_ERR_ARG, "tsmm_cn: %d x %d outputs above 256 x 32", k1, nc);
+    if (k1 > 256 || nc > 64 || (nc > 32 && k1 > 64))
+        return qd_set_error(QD_ERR_ARG, "tsmm_cn: %d x %d outputs (at most 256 x 32 or 64 x 64)", k1, nc);
     if (m <= 0) {
         CUDA_OK(cudaMemset2DAsync(C, sizeof(cpx<R>) * ldc, 0, sizeof(cpx<R>) * k1, nc, st));
         return QD_OK;
     }
     int rows, slices;
     cn_slices(m, &rows, &slices);
+    if ((size_t)slices * k1 * nc * sizeof(cpx<R>) > scratch_bytes)
+        return qd_set_error(QD_ERR_ARG, "tsmm_cn: scratch of %zu bytes below the %zu needed", scratch_bytes,
+                            (size_t)slices * k1 * nc * sizeof(cpx<R>));
     const int ku = (k1 + 31) / 32;
-    const size_t smem = sizeof(cpx<R>) * (size_t)CN_RC * (32 * ku + 1 + 33);
     qd_count_launch(2);
     int rc = QD_OK;
-    switch (ku) {
-        case 1: rc = cn_launch<R, 1>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 2: rc = cn_launch<R, 2>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 3: rc = cn_launch<R, 3>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 4: rc = cn_launch<R, 4>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 5: rc = cn_launch<R, 5>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 6: rc = cn_launch<R, 6>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        case 7: rc = cn_launch<R, 7>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
-        default: rc = cn_launch<R, 8>(slices, smem, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+    if (nc > 32) {
+        rc = ku == 1 ? cn_launch<R, 1, 64>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch)
+                     : cn_launch<R, 2, 64>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch);
+    } else {
+        switch (ku) {
+            case 1: rc = cn_launch<R, 1>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 2: rc = cn_launch<R, 2>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 3: rc = cn_launch<R, 3>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 4: rc = cn_launch<R, 4>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 5: rc = cn_launch<R, 5>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 6: rc = cn_launch<R, 6>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            case 7: rc = cn_launch<R, 7>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+            default: rc = cn_launch<R, 8>(slices, st, m, A, lda, k1, B, ldb, nc, rows, scratch); break;
+        }
     }
     if (rc) return rc;
     const int nout = k1 * nc;
@@ -310,11 +329,15 @@ int small_cn(int k, int n1, int n2, const cpx<R> *A, int lda, const cpx<R> *B, i
 
 }  // namespace
 
-// Partial-sum scratch (bytes) needed by qd_tsmm_cn for m rows and k1 x nc outputs.
+// Partial-sum scratch (bytes) that qd_tsmm_cn needs for any row count up to m
+// and k1 x nc outputs.  The slice count is not monotonic in m (slices are
+// rounded to whole shared-memory chunks), so the bound is taken over every
+// m' <= m: at most one slice per SM, and at most ceil(m / 64).
 extern "C" size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes) {
-    int rows, slices;
-    cn_slices(m > 0 ? m : 1, &rows, &slices);
-    return (size_t)slices * k1 * nc * elem_bytes;
+    int64_t smax = (int64_t)nsm();
+    const int64_t by_rows = ((int64_t)(m > 0 ? m : 1) + 63) / 64;
+    if (by_rows < smax) smax = by_rows;
+    return (size_t)smax * k1 * nc * elem_bytes;
 }
 
 // C-linkage entry points for both precisions (fp32 != 0: complex64).  Terms
@@ -338,13 +361,13 @@ extern "C" int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const
 }
 
 extern "C" int qd_tsmm_cn(int fp32, int m, const void *A, int64_t lda, int k1, const void *B, int64_t ldb, int nc,
-                          void *C, int64_t ldc, void *scratch, void *stream) {
+                          void *C, int64_t ldc, void *scratch, size_t scratch_bytes, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (fp32)
         return tsmm_cn<float>(m, (const cpx<float> *)A, lda, k1, (const cpx<float> *)B, ldb, nc, (cpx<float> *)C, ldc,
-                              (cpx<float> *)scratch, st);
+                              (cpx<float> *)scratch, scratch_bytes, st);
     return tsmm_cn<double>(m, (const cpx<double> *)A, lda, k1, (const cpx<double> *)B, ldb, nc, (cpx<double> *)C, ldc,
-                           (cpx<double> *)scratch, st);
+                           (cpx<double> *)scratch, scratch_bytes, st);
 }
 
 extern "C" int qd_small_cn(int fp32, int k, int n1, int n2, const void *A, int lda, const void *B, int ldb,

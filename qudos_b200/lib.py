@@ -114,7 +114,7 @@ _sig("qd_tc_kernel_stats", ci, [ci, C.POINTER(C.c_longlong), C.POINTER(C.c_doubl
 _sig("qd_gemm_peak", ci, [ci, ci, ci, C.POINTER(C.c_double)])
 _sig("qd_tsmm_nn", ci, [ci, ci, ci, ci, C.POINTER(vp), C.POINTER(i64), C.POINTER(vp), C.POINTER(i64), C.POINTER(ci),
                         C.POINTER(ci), C.POINTER(C.c_double), vp, i64, C.c_double, vp])
-_sig("qd_tsmm_cn", ci, [ci, ci, vp, i64, ci, vp, i64, ci, vp, i64, vp, vp])
+_sig("qd_tsmm_cn", ci, [ci, ci, vp, i64, ci, vp, i64, ci, vp, i64, vp, C.c_size_t, vp])
 _sig("qd_small_cn", ci, [ci, ci, ci, ci, vp, ci, vp, ci, C.c_double, vp, ci, vp])
 _sig("qd_tsmm_cn_scratch_bytes", C.c_size_t, [ci, ci, ci, ci])
 _sig("qd_set_wait_limits", ci, [C.c_longlong, C.c_longlong, C.c_longlong])

@@ -42,7 +42,8 @@ def _tol(dtype):
 
 @pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
 @pytest.mark.parametrize("m,nc,K0,K1,bt", [(1000, 32, 64, 64, 1), (27000, 32, 224, 224, 1), (333, 7, 5, 0, 0),
-                                           (5000, 32, 32, 0, 0), (129, 32, 256, 256, 0)])
+                                           (5000, 32, 32, 0, 0), (129, 32, 256, 256, 0), (27000, 48, 32, 0, 0),
+                                           (2000, 64, 40, 40, 1)])
 def test_tsmm_nn(dtype, m, nc, K0, K1, bt):
     rng = np.random.default_rng(m + nc + K0)
     A0, A1 = _rnd(rng, (m, K0), dtype), _rnd(rng, (m, max(K1, 1)), dtype)
@@ -73,7 +74,8 @@ def test_tsmm_nn(dtype, m, nc, K0, K1, bt):
 
 
 @pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
-@pytest.mark.parametrize("m,k1,nc", [(27000, 32, 32), (27000, 224, 32), (100, 256, 5), (64, 17, 32), (7000, 96, 20)])
+@pytest.mark.parametrize("m,k1,nc", [(27000, 32, 32), (27000, 224, 32), (100, 256, 5), (64, 17, 32), (7000, 96, 20),
+                                     (27000, 32, 48), (9472, 64, 64), (3000, 40, 33)])
 def test_tsmm_cn(dtype, m, k1, nc):
     rng = np.random.default_rng(m + k1 + nc)
     A, B = _rnd(rng, (m, k1), dtype), _rnd(rng, (m, nc), dtype)
@@ -82,8 +84,10 @@ def test_tsmm_cn(dtype, m, k1, nc):
     scale = np.abs(A2).T @ np.abs(B2)
     dA, dB, dC = _dev(A), _dev(B), L.DeviceBuffer(16 * k1 * nc)
     es = 8 if dtype == np.complex64 else 16
-    scr = L.DeviceBuffer(L.lib.qd_tsmm_cn_scratch_bytes(m, k1, nc, es))
-    L.check(L.lib.qd_tsmm_cn(int(dtype == np.complex64), m, dA.ptr, m, k1, dB.ptr, m, nc, dC.ptr, k1, scr.ptr, None))
+    nbytes = L.lib.qd_tsmm_cn_scratch_bytes(m, k1, nc, es)
+    scr = L.DeviceBuffer(nbytes)
+    L.check(L.lib.qd_tsmm_cn(int(dtype == np.complex64), m, dA.ptr, m, k1, dB.ptr, m, nc, dC.ptr, k1, scr.ptr, nbytes,
+                             None))
     got = _get(dC, (k1, nc), dtype)
     assert (np.abs(got - ref) / scale).max() < _tol(dtype)
 
@@ -124,3 +128,11 @@ def test_hemm_gram_zgemm(n, k):
     L.check(L.lib.qd_zgemm_small_dev(n, dX.ptr, n, k, dCm.ptr, k, k, dZ.ptr, n, -1.0, None))
     Z = _get(dZ, (n, k), np.complex128)
     assert np.abs(Z - (X @ Cm - Y0)).max() < 1e-12 * np.abs(X @ Cm).max()
+
+
+def test_tsmm_cn_rejects_small_scratch():
+    m, k1, nc = 9472, 32, 32
+    dA, dB, dC = L.DeviceBuffer(8 * m * k1), L.DeviceBuffer(8 * m * nc), L.DeviceBuffer(8 * k1 * nc)
+    scr = L.DeviceBuffer(1024)
+    rc = L.lib.qd_tsmm_cn(1, m, dA.ptr, m, k1, dB.ptr, m, nc, dC.ptr, k1, scr.ptr, 1024, None)
+    assert rc == L.QD_ERR_ARG
