@@ -66,6 +66,6 @@ def test_momentum_matrix_elements(name, tmp_path):
     assert np.abs(mref - got).max() <= 1e-12 * np.abs(got).max()
     write_momentum_matrix_elements(str(tmp_path), got)
     rows = np.loadtxt(os.path.join(str(tmp_path), "momentum_matrix_elements.dat"))
-    assert rows.shape == (nc * nv, 2 + 9)
+    assert rows.shape == (nc * nv, 2 + 15)  # [100], [010], [001], [110], [-110]
     hb = np.sqrt(7.61996 / 2.0)
     assert np.allclose(rows[:, 4], np.abs(got[0]).reshape(-1) / hb, rtol=1e-9, atol=0)
