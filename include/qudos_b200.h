@@ -413,7 +413,7 @@ int qd_residual_norms_dev(int64_t n, const void *R, int64_t ldr, const void *Z, 
  *               scratch_bytes >= qd_tsmm_cn_scratch_bytes(m, k1, nc, 8 or 16)
  *               of partial sums (QD_ERR_ARG when too small), which are
  *               added in FP64 in a fixed order;
- *   qd_small_cn C[n1 x n2] = alpha A^H B for small k x n1, k x n2 inputs. */
+ *   qd_small_cn C[n1 x n2] = alpha A^H B for k x n1, k x n2 inputs, k, n1, n2 <= 32. */
 int qd_tsmm_nn(int fp32, int m, int nc, int nterms, const void *const *A, const int64_t *lda, const void *const *B,
                const int64_t *ldb, const int *K, const int *btrans, const double *alpha, void *C, int64_t ldc,
                double beta, void *stream);

@@ -18,7 +18,7 @@
 //            the partials in FP64 (a fixed order, so results do not depend on
 //            scheduling).  Serves the Gram matrix V^H V, [W V]^H VT, V^H X and
 //            V^H Z.
-//   small_cn C[n1 x n2] = A[k x n1]^H B[k x n2] for small matrices (T^H M).
+//   small_cn C[n1 x n2] = A[k x n1]^H B[k x n2] for matrices of up to 32 x 32 (T^H M).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -54,64 +54,88 @@ __device__ __forceinline__ cpx<R> cfma_(cpx<R> acc, cpx<R> a, cpx<R> b) {
     return acc;
 }
 
-constexpr int NN_TM = 128;
-
-// Thread (tx, ty): rows tx + 32 i (i < 4), columns NJ ty + j (j < NJ), NJ =
-// NCW / 8 for an output width of NCW = 32 or 64 columns.
-template <typename R, int NCW>
+// Thread (tx, ty): rows tx + 32 i (i < RI, a tile of 32 RI rows), columns
+// NJ ty + j (j < NJ), NJ = NCW / 8 for an output width of NCW = 32 or 64.
+// The K dimension of both terms is one sequence of chunks; the next chunk's
+// global loads are issued into registers before the current chunk is
+// multiplied, so their latency overlaps the arithmetic.
+template <typename R, int NCW, int RI>
 __global__ void __launch_bounds__(256) tsmm_nn_kernel(int m, int nc, TsTerm<R> t0, TsTerm<R> t1, int nterms,
                                                       cpx<R> *C, int64_t ldc, R beta) {
     // K chunk of 16 (8 for complex128 at 64 columns, to stay within 48 KB of static shared memory)
-    constexpr int NN_NC = NCW, NJ = NCW / 8, NN_KC = (sizeof(R) == 8 && NCW == 64) ? 8 : 16;
-    __shared__ cpx<R> As[NN_KC][NN_TM];
-    __shared__ cpx<R> Bs[NN_KC][NN_NC + 1];
+    constexpr int TM = 32 * RI, NJ = NCW / 8, KC = (sizeof(R) == 8 && NCW == 64) ? 8 : 16;
+    constexpr int LA = KC * TM / 256, LB = (KC * NCW + 255) / 256;
+    __shared__ cpx<R> As[KC][TM];
+    __shared__ cpx<R> Bs[KC][NCW + 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int r0 = blockIdx.x * NN_TM;
-    cpx<R> acc[4][NJ];
+    const int r0 = blockIdx.x * TM;
+    const int nch0 = (t0.K + KC - 1) / KC, nch = nch0 + (nterms > 1 ? (t1.K + KC - 1) / KC : 0);
+    cpx<R> acc[RI][NJ];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < RI; i++)
 #pragma unroll
         for (int j = 0; j < NJ; j++) acc[i][j] = mk<R>(0, 0);
-    for (int t = 0; t < nterms; t++) {
-        const TsTerm<R> &T = t == 0 ? t0 : t1;
-        for (int p0 = 0; p0 < T.K; p0 += NN_KC) {
-            for (int e = threadIdx.x; e < NN_KC * NN_TM; e += 256) {
-                const int r = e % NN_TM, p = e / NN_TM;
-                const int gr = r0 + r, gp = p0 + p;
-                As[p][r] = (gr < m && gp < T.K) ? T.A[gr + (int64_t)gp * T.lda] : mk<R>(0, 0);
-            }
-            for (int e = threadIdx.x; e < NN_KC * NN_NC; e += 256) {
-                cpx<R> v = mk<R>(0, 0);
-                int p, c;
+    cpx<R> ra[LA], rb[LB];
+    auto fetch = [&](int ch) {
+        const TsTerm<R> &T = ch < nch0 ? t0 : t1;
+        const int p0 = (ch < nch0 ? ch : ch - nch0) * KC;
+#pragma unroll
+        for (int l = 0; l < LA; l++) {
+            const int e = threadIdx.x + 256 * l;
+            const int r = e % TM, p = e / TM;
+            const int gr = r0 + r, gp = p0 + p;
+            ra[l] = (gr < m && gp < T.K) ? T.A[gr + (int64_t)gp * T.lda] : mk<R>(0, 0);
+        }
+#pragma unroll
+        for (int l = 0; l < LB; l++) {
+            const int e = threadIdx.x + 256 * l;
+            cpx<R> v = mk<R>(0, 0);
+            if (e < KC * NCW) {
                 if (!T.btrans) {
-                    p = e % NN_KC;
-                    c = e / NN_KC;
+                    const int p = e % KC, c = e / KC;
                     if (p0 + p < T.K && c < nc) v = T.B[(p0 + p) + (int64_t)c * T.ldb];
                 } else {
-                    c = e % NN_NC;
-                    p = e / NN_NC;
+                    const int c = e % NCW, p = e / NCW;
                     if (p0 + p < T.K && c < nc) v = cconj(T.B[c + (int64_t)(p0 + p) * T.ldb]);
                 }
-                Bs[p][c] = mk<R>(T.alpha * v.re, T.alpha * v.im);
             }
-            __syncthreads();
+            rb[l] = mk<R>(T.alpha * v.re, T.alpha * v.im);
+        }
+    };
+    if (nch > 0) fetch(0);
+    for (int ch = 0; ch < nch; ch++) {
+        __syncthreads();
+#pragma unroll
+        for (int l = 0; l < LA; l++) {
+            const int e = threadIdx.x + 256 * l;
+            As[e / TM][e % TM] = ra[l];
+        }
+        const TsTerm<R> &T = ch < nch0 ? t0 : t1;
+#pragma unroll
+        for (int l = 0; l < LB; l++) {
+            const int e = threadIdx.x + 256 * l;
+            if (e < KC * NCW) {
+                if (!T.btrans) Bs[e % KC][e / KC] = rb[l];
+                else Bs[e / NCW][e % NCW] = rb[l];
+            }
+        }
+        __syncthreads();
+        if (ch + 1 < nch) fetch(ch + 1);
 #pragma unroll 4
-            for (int p = 0; p < NN_KC; p++) {
-                cpx<R> a[4], b[NJ];
+        for (int p = 0; p < KC; p++) {
+            cpx<R> a[RI], b[NJ];
 #pragma unroll
-                for (int i = 0; i < 4; i++) a[i] = As[p][tx + 32 * i];
+            for (int i = 0; i < RI; i++) a[i] = As[p][tx + 32 * i];
 #pragma unroll
-                for (int j = 0; j < NJ; j++) b[j] = Bs[p][NJ * ty + j];
+            for (int j = 0; j < NJ; j++) b[j] = Bs[p][NJ * ty + j];
 #pragma unroll
-                for (int i = 0; i < 4; i++)
+            for (int i = 0; i < RI; i++)
 #pragma unroll
-                    for (int j = 0; j < NJ; j++) acc[i][j] = cfma_(acc[i][j], a[i], b[j]);
-            }
-            __syncthreads();
+                for (int j = 0; j < NJ; j++) acc[i][j] = cfma_(acc[i][j], a[i], b[j]);
         }
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < RI; i++) {
         const int gr = r0 + tx + 32 * i;
         if (gr >= m) continue;
 #pragma unroll
@@ -210,15 +234,20 @@ __global__ void __launch_bounds__(256) cn_reduce_kernel(const cpx<R> *__restrict
     if (lane == 0) C[(o % k1) + (int64_t)(o / k1) * ldc] = mk<R>((R)sr, (R)si);
 }
 
-// C[n1 x n2] = alpha A[k x n1]^H B[k x n2], small (one CTA, FP64 sums).
+// C[n1 x n2] = alpha A[k x n1]^H B[k x n2], small (one CTA; k, n1, n2 <= 32;
+// both factors staged in shared memory, FP64 sums).
 template <typename R>
-__global__ void small_cn_kernel(int k, int n1, int n2, const cpx<R> *A, int lda, const cpx<R> *B, int ldb, R alpha,
-                                cpx<R> *C, int ldc) {
+__global__ void __launch_bounds__(1024) small_cn_kernel(int k, int n1, int n2, const cpx<R> *A, int lda,
+                                                        const cpx<R> *B, int ldb, R alpha, cpx<R> *C, int ldc) {
+    __shared__ cpx<R> As[32][33], Bs[32][33];
+    for (int e = threadIdx.x; e < k * n1; e += blockDim.x) As[e / k][e % k] = A[(e % k) + (e / k) * lda];
+    for (int e = threadIdx.x; e < k * n2; e += blockDim.x) Bs[e / k][e % k] = B[(e % k) + (e / k) * ldb];
+    __syncthreads();
     for (int o = threadIdx.x; o < n1 * n2; o += blockDim.x) {
         const int i = o % n1, j = o / n1;
         double sr = 0.0, si = 0.0;
         for (int p = 0; p < k; p++) {
-            const cpx<R> a = A[p + i * lda], b = B[p + j * ldb];
+            const cpx<R> a = As[i][p], b = Bs[j][p];
             sr += (double)a.re * b.re + (double)a.im * b.im;
             si += (double)a.re * b.im - (double)a.im * b.re;
         }
@@ -237,10 +266,12 @@ int nsm() {
     return g_nsm;
 }
 
-// Rows per slice and slice count of tsmm_cn for m rows: one wave of at most
-// one CTA per SM, at least 64 rows each.
-void cn_slices(int m, int *rows, int *slices) {
-    int s = nsm();
+// Rows per slice and slice count of tsmm_cn for m rows and k1 outputs per
+// column: up to four CTAs per SM for narrow products (so that loads of some
+// CTAs overlap the arithmetic of others), one for the widest, at least 64
+// rows each.
+void cn_slices(int m, int k1, int *rows, int *slices) {
+    int s = nsm() * (k1 <= 64 ? 4 : k1 <= 128 ? 2 : 1);
     int r = (m + s - 1) / s;
     if (r < 64) r = 64;
     r = ((r + CN_RC - 1) / CN_RC) * CN_RC;
@@ -254,11 +285,20 @@ int tsmm_nn(int m, int nc, int nterms, const TsTerm<R> *terms, cpx<R> *C, int64_
     if (nc > 64) return qd_set_error(QD_ERR_ARG, "tsmm_nn: %d columns above 64", nc);
     TsTerm<R> t1 = nterms > 1 ? terms[1] : terms[0];
     qd_count_launch(1);
-    const unsigned grid = (unsigned)((m + NN_TM - 1) / NN_TM);
-    if (nc <= 32)
-        tsmm_nn_kernel<R, 32><<<grid, 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta);
-    else
-        tsmm_nn_kernel<R, 64><<<grid, 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta);
+    // rows per CTA: 128 while that still gives two CTAs per SM, else 64 or 32
+    const int ri = m >= 2 * 128 * nsm() ? 4 : m >= 2 * 64 * nsm() ? 2 : 1;
+    const unsigned grid = (unsigned)((m + 32 * ri - 1) / (32 * ri));
+#define QD_NN(W, RI) tsmm_nn_kernel<R, W, RI><<<grid, 256, 0, st>>>(m, nc, terms[0], t1, nterms, C, ldc, beta)
+    if (nc <= 32) {
+        if (ri == 4) QD_NN(32, 4);
+        else if (ri == 2) QD_NN(32, 2);
+        else QD_NN(32, 1);
+    } else {
+        if (ri == 4) QD_NN(64, 4);
+        else if (ri == 2) QD_NN(64, 2);
+        else QD_NN(64, 1);
+    }
+#undef QD_NN
     CUDA_OK(cudaGetLastError());
     return QD_OK;
 }
@@ -289,7 +329,7 @@ int tsmm_cn(int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B, int64_
         return QD_OK;
     }
     int rows, slices;
-    cn_slices(m, &rows, &slices);
+    cn_slices(m, k1, &rows, &slices);
     if ((size_t)slices * k1 * nc * sizeof(cpx<R>) > scratch_bytes)
         return qd_set_error(QD_ERR_ARG, "tsmm_cn: scratch of %zu bytes below the %zu needed", scratch_bytes,
                             (size_t)slices * k1 * nc * sizeof(cpx<R>));
@@ -321,6 +361,8 @@ int tsmm_cn(int m, const cpx<R> *A, int64_t lda, int k1, const cpx<R> *B, int64_
 template <typename R>
 int small_cn(int k, int n1, int n2, const cpx<R> *A, int lda, const cpx<R> *B, int ldb, R alpha, cpx<R> *C, int ldc,
              cudaStream_t st) {
+    if (k < 1 || n1 < 1 || n2 < 1 || k > 32 || n1 > 32 || n2 > 32)
+        return qd_set_error(QD_ERR_ARG, "small_cn: sizes above 32");
     qd_count_launch(1);
     small_cn_kernel<R><<<1, 1024, 0, st>>>(k, n1, n2, A, lda, B, ldb, alpha, C, ldc);
     CUDA_OK(cudaGetLastError());
@@ -330,11 +372,12 @@ int small_cn(int k, int n1, int n2, const cpx<R> *A, int lda, const cpx<R> *B, i
 }  // namespace
 
 // Partial-sum scratch (bytes) that qd_tsmm_cn needs for any row count up to m
-// and k1 x nc outputs.  The slice count is not monotonic in m (slices are
-// rounded to whole shared-memory chunks), so the bound is taken over every
-// m' <= m: at most one slice per SM, and at most ceil(m / 64).
+// and any product of at most k1 x nc outputs.  The slice count is not
+// monotonic in m (slices are rounded to whole shared-memory chunks), so the
+// bound is taken over every m' <= m: at most four slices per SM, and at most
+// ceil(m / 64).
 extern "C" size_t qd_tsmm_cn_scratch_bytes(int m, int k1, int nc, int elem_bytes) {
-    int64_t smax = (int64_t)nsm();
+    int64_t smax = 4 * (int64_t)nsm();
     const int64_t by_rows = ((int64_t)(m > 0 ? m : 1) + 63) / 64;
     if (by_rows < smax) smax = by_rows;
     return (size_t)smax * k1 * nc * elem_bytes;
