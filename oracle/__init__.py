@@ -13,9 +13,12 @@ against the reference's own golden outputs
 (``code/example/Prism_111/Electronic_structure/PWEM_test_ref/energies_*.dat``),
 which cover the closed-form shapes, anisotropic strain, first- and
 second-order piezoelectricity, the identity strain-cell downsampling, the
-assembly block map and the index-window eigensolve.  The lens shape transform
-(``I_J0`` quadrature) has no golden file in the reference and is pinned only
-against an independent adaptive quadrature (see ``shapes.i_j0``).
+assembly block map and the index-window eigensolve, plus the example's
+Coulomb, momentum-matrix-element and probability-density outputs.  The lens
+shape transform has no golden file in the reference; its integral ``I_J0`` is
+evaluated the way the reference evaluates it, by GSL's adaptive 61-point
+Gauss-Kronrod routine, restated in ``quadrature`` (GSL itself is an external
+library that is not part of the checkout).
 """
 
 from . import inputs, materials, shapes, strain, hamiltonian, eigen, coulomb, pipeline  # noqa: F401

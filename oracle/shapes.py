@@ -38,21 +38,32 @@ def sinc_pi(x):
     return float(np.sinc(x))
 
 
-# Gauss-Legendre rule for I_J0 (see i_j0)
+# Gauss-Legendre rule for the cross-check of I_J0 (i_j0_gauss_legendre)
 _GL_X, _GL_W = np.polynomial.legendre.leggauss(96)
 _GL_X = 0.5 * (_GL_X + 1.0)
 _GL_W = 0.5 * _GL_W
 
 
+def _i_j0_integrand(alpha, beta):
+    return lambda x: x * np.cos(alpha * np.sqrt(np.maximum(1.0 - x * x, 0.0))) * j0(beta * x)
+
+
 def i_j0(alpha, beta):
-    """I_J0(alpha, beta) = int_0^1 x cos(alpha sqrt(1-x^2)) J0(beta x) dx
-    (characteristic_function_fourier_integrals.c:107-153, GSL QAG key 6 with
-    EPS_ABS = EPS_REL = 1e-4).  cos(alpha sqrt(1-x^2)) is a power series in
-    (1 - x^2), so the integrand is entire and QAG's first 61-point Kronrod pass
-    already converges to rounding for the |alpha|, |beta| <= ~40 met by these
-    grids; a 96-point Gauss-Legendre rule gives the same value."""
+    """I_J0(alpha, beta) = int_0^1 x cos(alpha sqrt(1-x^2)) J0(beta x) dx by the
+    reference's method: gsl_integration_qag with the 61-point Gauss-Kronrod
+    rule and EPS_ABS = EPS_REL = 1e-4, LIMIT = 1000
+    (characteristic_function_fourier_integrals.c:107-153, 8_band.h:61-63),
+    restated in ``quadrature.qag61``."""
+    from .quadrature import qag61
+    return qag61(_i_j0_integrand(alpha, beta), 0.0, 1.0, 1.0e-4, 1.0e-4, 1000)[0]
+
+
+def i_j0_gauss_legendre(alpha, beta):
+    """The same integral by a 96-point Gauss-Legendre rule (the rule the CUDA
+    table kernel uses); cos(alpha sqrt(1-x^2)) is a power series in (1 - x^2),
+    so the integrand is entire and both rules converge to rounding."""
     x = _GL_X
-    return float(np.sum(_GL_W * x * np.cos(alpha * np.sqrt(1.0 - x * x)) * j0(beta * x)))
+    return float(np.sum(_GL_W * _i_j0_integrand(alpha, beta)(x)))
 
 
 def i_e0(a, G):

@@ -257,9 +257,12 @@ __global__ void __launch_bounds__(256) panel_qr_kernel(cpx<R> *A, int64_t lda, i
 }
 
 // T of the compact WY form (LAPACK zlarft, forward, columnwise):
-// T[i,i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i].  One block;
-// the Gram matrix is staged in shared memory first (dynamic: 2 nb^2 double2),
-// so the sequential recursion over i never waits on global memory.
+// T[i,i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i].  One block of
+// nb <= 32 warps; the Gram matrix is staged in shared memory first (dynamic:
+// 2 nb^2 double2).  Column i depends on the columns before it, so the columns
+// are formed in order, but each entry T[p, i] of a column is one warp's
+// shuffle-reduced dot product over q in [p, i), so a column costs one reduction
+// and one block barrier instead of a serial loop per thread.
 template <typename R>
 __global__ void form_t_kernel(const cpx<R> *gram, int ldg, const cpx<R> *tau, cpx<R> *T, int ldt, int nb) {
     extern __shared__ double2 ft_smem[];
@@ -272,16 +275,25 @@ __global__ void form_t_kernel(const cpx<R> *gram, int ldg, const cpx<R> *tau, cp
         Gs[idx] = make_double2((double)g.re, (double)g.im);
     }
     __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = 1; i < nb; i++) {
-        const double2 t = Tl[i + i * nb];
-        for (int p = threadIdx.x; p < i; p += blockDim.x) {
+        if (w < i) {  // entry p = w of column i
+            const int p = w;
+            const int q = p + lane;
             double sr = 0.0, si = 0.0;
-            for (int q = p; q < i; q++) {
+            if (q < i) {
                 const double2 a = Tl[p + q * nb], g = Gs[q + i * nb];
-                sr += a.x * g.x - a.y * g.y;
-                si += a.x * g.y + a.y * g.x;
+                sr = a.x * g.x - a.y * g.y;
+                si = a.x * g.y + a.y * g.x;
             }
-            Tl[p + i * nb] = make_double2(-(t.x * sr - t.y * si), -(t.x * si + t.y * sr));
+            for (int o = 16; o > 0; o >>= 1) {
+                sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                si += __shfl_xor_sync(0xffffffffu, si, o);
+            }
+            if (lane == 0) {
+                const double2 t = Tl[i + i * nb];
+                Tl[p + i * nb] = make_double2(-(t.x * sr - t.y * si), -(t.x * si + t.y * sr));
+            }
         }
         __syncthreads();
     }
@@ -543,7 +555,7 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
                 ft_configured[ti] = 1;
             }
         }
-        form_t_kernel<R><<<1, 256, 2 * nb * nb * sizeof(double2), st>>>((const cpx<R> *)w.gram, b,
+        form_t_kernel<R><<<1, 32 * nb, 2 * nb * nb * sizeof(double2), st>>>((const cpx<R> *)w.gram, b,
                                                                         (const cpx<R> *)w.tau, (cpx<R> *)Tp, b, nb);
         CUDA_OK(cudaGetLastError());
         // 4. VT = V T ; 5. X = A22 VT (stale A22 + pending terms), written straight into Wacc
@@ -654,7 +666,7 @@ extern "C" void qd_stage1_free(Stage1Work *w, cudaStream_t st) {
 
 extern "C" int qd_stage1_run(void *A, int64_t n, int64_t lda, int b, int fp32, Stage1Work *w, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    if (b > 48) return qd_set_error(QD_ERR_UNSUPPORTED, "band width above 48");
+    if (b > 32) return qd_set_error(QD_ERR_UNSUPPORTED, "band width above 32");
     int rc = fp32 ? stage1<cuComplex>((cuComplex *)A, n, lda, b, *w, st)
                   : stage1<cuDoubleComplex>((cuDoubleComplex *)A, n, lda, b, *w, st);
     if (rc) return rc;

@@ -110,3 +110,16 @@ def test_prism_111_probability_densities_match_golden(prism_solution):
         for ours, ref in ((vb, gold["vb_" + tag]), (cb, gold["cb_" + tag])):
             # 7 significant digits in the files
             assert np.all(np.abs(ours - ref) <= 1e-5 * np.abs(ref).max() + 2e-6 * np.abs(ref)), tag
+
+
+def test_lens_integral_qag_restatement_matches_gauss_legendre():
+    """The lens integral I_J0 by the restated GSL QAG (61-point Kronrod rule,
+    the reference's method) and by the 96-point Gauss-Legendre rule of the CUDA
+    table kernel, over the (alpha, beta) range of the lens decks' grids and
+    beyond (|alpha| <= 40, |beta| <= 60): agreement to 1e-13."""
+    from oracle import shapes
+    rng = np.random.default_rng(11)
+    for alpha, beta in rng.uniform([-40.0, 0.0], [40.0, 60.0], size=(400, 2)):
+        a = shapes.i_j0(alpha, beta)
+        b = shapes.i_j0_gauss_legendre(alpha, beta)
+        assert abs(a - b) <= 1e-13, (alpha, beta, a, b)
