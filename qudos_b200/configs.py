@@ -74,9 +74,11 @@ def pyramid_11(mg=5, n_states=8, cme=1, height=5.0, half_base=9.0, x=0.4, fz=10.
     return params, cell
 
 
-def molecule_15(mg=7, n_states=8):
+def molecule_15(mg=7, n_states=8, cme=0):
+    """The benchmark deck; cme > 0 also asks for Coulomb matrix elements on a
+    Coulomb cell equal to the electronic cell (mg plane waves per axis)."""
     params = parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg, M_S_Gy=mg, M_S_Gz=mg, N_VB=n_states,
-                             N_CB=n_states, Piezo=1)
+                             N_CB=n_states, Piezo=1, CME=cme, M_C_Gx=mg, M_C_Gy=mg, M_C_Gz=mg)
     cell = (supercell_record((40.0, 40.0, 32.0)) +
             shape_record(4, 3, 0.5, 0.0, (0.0, 0.0, -5.25), (9.0, 9.0, 3.0)) +
             shape_record(4, 3, 0.5, 0.0, (0.0, 0.0, 1.75), (10.0, 10.0, 3.5)))

@@ -12,13 +12,13 @@
 //   4. B on the Coulomb-cell grid: a scaled copy when the cells agree, else
 //      separable sinc weights per axis (B_coulomb_supercell.c:23-139);
 //   5. w(G) times the reversed B (coulomb_matrix_elements.c:370-401, 498-503);
-//   6. every pair-pair contraction at once as two complex GEMMs over the grid
+//   6. every pair-pair contraction at once as two reductions over the grid
 //      (sum Brw_q B_p and sum conj(Brw_q) B_p), and the dipole/quadrupole
-//      moments as one more (cuBLAS: plain library GEMMs);
+//      moments as two more, in the library's FP64 Gram kernel
+//      (eig_refine.cu: row slices, 64 x 64 output tiles);
 //   7. on the host: the Madelung constant and the reference's symmetry-reduced
 //      index loops (coulomb_integrals.c:23-356), which pick entries of those
 //      matrices and add the CME >= 2 corrections.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -31,7 +31,8 @@
 #include "qd_internal.h"
 
 extern "C" int qd_dft3_batched(double2 *d, int64_t stride_b, int nb, const int n[3], int sign, void *stream);
-extern "C" cublasHandle_t qd_cublas(void);
+extern "C" int qd_gram_ex_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb,
+                              void *C, int ldc, int conj_a, void *stream);
 
 #define CUDA_OK(x)                                                                                    \
     do {                                                                                              \
@@ -39,13 +40,6 @@ extern "C" cublasHandle_t qd_cublas(void);
         if (e_ != cudaSuccess)                                                                        \
             return qd_set_error(QD_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
     } while (0)
-#define BLAS_OK(x)                                                                                   \
-    do {                                                                                             \
-        cublasStatus_t s_ = (x);                                                                     \
-        if (s_ != CUBLAS_STATUS_SUCCESS)                                                             \
-            return qd_set_error(QD_ERR_CUDA, "%s:%d cuBLAS status %d", __FILE__, __LINE__, (int)s_); \
-    } while (0)
-
 typedef std::complex<double> cd;
 
 namespace {
@@ -392,29 +386,17 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
     qd_count_launch(1);
     coulomb_reverse_kernel<<<blocks_for(SC * P), 256, 0, st>>>(BC, SC, P, wd, Brw);
     RCK(cudaGetLastError());
-    // 6: contractions
-    cublasHandle_t h = qd_cublas();
-    if (!h) {
-        release();
-        return qd_set_error(QD_ERR_CUDA, "cuBLAS unavailable");
-    }
-    const cuDoubleComplex one = {1, 0}, zero = {0, 0};
-    cublasStatus_t bs = cublasSetStream(h, st ? st : cudaStreamPerThread);
-    if (bs == CUBLAS_STATUS_SUCCESS)
-        bs = cublasZgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, P, P, (int)SC, &one, (const cuDoubleComplex *)Brw, (int)SC,
-                         (const cuDoubleComplex *)BC, (int)SC, &zero, (cuDoubleComplex *)U, P);
-    if (bs == CUBLAS_STATUS_SUCCESS)
-        bs = cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, P, P, (int)SC, &one, (const cuDoubleComplex *)Brw, (int)SC,
-                         (const cuDoubleComplex *)BC, (int)SC, &zero, (cuDoubleComplex *)Cc, P);
-    if (bs == CUBLAS_STATUS_SUCCESS)
-        bs = cublasZgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, P, 4, (int)SC, &one, (const cuDoubleComplex *)BC, (int)SC,
-                         (const cuDoubleComplex *)V4, (int)SC, &zero, (cuDoubleComplex *)Dm, P);
-    if (bs == CUBLAS_STATUS_SUCCESS)
-        bs = cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, P, 4, (int)SC, &one, (const cuDoubleComplex *)BC, (int)SC,
-                         (const cuDoubleComplex *)V4, (int)SC, &zero, (cuDoubleComplex *)Dc, P);
-    if (bs != CUBLAS_STATUS_SUCCESS) {
-        release();
-        return qd_set_error(QD_ERR_CUDA, "qd_coulomb: cuBLAS status %d", (int)bs);
+    // 6: contractions over the Coulomb grid (coulomb_integrals.c:62-142 as four products):
+    //    U = Brw^T BC, Cc = Brw^H BC, Dm = BC^T V4, Dc = BC^H V4
+    {
+        int rc = qd_gram_ex_dev(SC, Brw, SC, P, BC, SC, P, U, P, 0, st);
+        if (rc == QD_OK) rc = qd_gram_ex_dev(SC, Brw, SC, P, BC, SC, P, Cc, P, 1, st);
+        if (rc == QD_OK) rc = qd_gram_ex_dev(SC, BC, SC, P, V4, SC, 4, Dm, P, 0, st);
+        if (rc == QD_OK) rc = qd_gram_ex_dev(SC, BC, SC, P, V4, SC, 4, Dc, P, 1, st);
+        if (rc != QD_OK) {
+            release();
+            return rc;
+        }
     }
     std::vector<cd> Uh((size_t)P * P), Ch((size_t)P * P), Dmh((size_t)P * 4), Dch((size_t)P * 4);
     RCK(cudaMemcpyAsync(Uh.data(), U, zsz * P * P, cudaMemcpyDeviceToHost, st));

@@ -138,10 +138,12 @@ __global__ void __launch_bounds__(HM_THREADS) hemm_lower_kernel(const double2 *_
     }
 }
 
-// C[0:ka, 0:kb] += A^H B over rows [slice), A n x ka, B n x kb (ka, kb <= 64).
+// C[0:ka, 0:kb] += A^H B (or A^T B with CONJ_A false) over rows [slice),
+// A n x ka, B n x kb (ka, kb <= 64).
 // The slice's rows go through shared memory 16 at a time; thread t owns the
 // outputs t, t + 256, ... of the ka x kb result.
 constexpr int GR_ROWS = 16;
+template <bool CONJ_A>
 __global__ void __launch_bounds__(256) gram_kernel(const double2 *__restrict__ A, int64_t lda, int ka,
                                                    const double2 *__restrict__ B, int64_t ldb, int kb, int n,
                                                    int rows_per_cta, double *__restrict__ C /* interleaved re, im */,
@@ -170,7 +172,9 @@ __global__ void __launch_bounds__(256) gram_kernel(const double2 *__restrict__ A
                 double2 s = acc[q];
 #pragma unroll 8
                 for (int r = 0; r < GR_ROWS; r++) {
-                    const double2 a = As[r][i], b = Bs[r][j];  // conj(a) b
+                    double2 a = As[r][i];
+                    const double2 b = Bs[r][j];  // conj(a) b, or a b
+                    if (!CONJ_A) a.y = -a.y;
                     s.x = fma(a.x, b.x, s.x);
                     s.x = fma(a.y, b.y, s.x);
                     s.y = fma(a.x, b.y, s.y);
@@ -294,10 +298,11 @@ extern "C" int qd_hemm_lower_dev(int64_t n, const void *H, int64_t ld, const voi
     return QD_OK;
 }
 
-// C (ka x kb, ldc, device, complex128) = A^H B over n rows; C is overwritten.
-// Output blocks of up to 64 x 64 are reduced one launch each.
-extern "C" int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb, void *C,
-                           int ldc, void *stream) {
+// C (ka x kb, ldc, device, complex128) = A^H B (conj_a != 0) or A^T B over n
+// rows; C is overwritten.  Output blocks of up to 64 x 64 are reduced one
+// launch each.
+extern "C" int qd_gram_ex_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb,
+                              void *C, int ldc, int conj_a, void *stream) {
     if (n < 1 || ka < 1 || kb < 1 || ldc < ka || n > 0x7fffffff) return qd_set_error(QD_ERR_ARG, "qd_gram_dev: bad sizes");
     cudaStream_t st = (cudaStream_t)stream;
     CUDA_OK(cudaMemset2DAsync(C, sizeof(double2) * (size_t)ldc, 0, sizeof(double2) * (size_t)ka, kb, st));
@@ -311,13 +316,22 @@ extern "C" int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const 
     for (int j0 = 0; j0 < kb; j0 += 64)
         for (int i0 = 0; i0 < ka; i0 += 64) {
             const int kai = ka - i0 < 64 ? ka - i0 : 64, kbj = kb - j0 < 64 ? kb - j0 : 64;
+            const double2 *Ab = (const double2 *)A + (int64_t)i0 * lda, *Bb = (const double2 *)B + (int64_t)j0 * ldb;
+            double *Cb = (double *)((double2 *)C + i0 + (int64_t)j0 * ldc);
             qd_count_launch(1);
-            gram_kernel<<<grid, 256, 0, st>>>((const double2 *)A + (int64_t)i0 * lda, lda, kai,
-                                              (const double2 *)B + (int64_t)j0 * ldb, ldb, kbj, (int)n, (int)rows,
-                                              (double *)((double2 *)C + i0 + (int64_t)j0 * ldc), ldc);
+            if (conj_a)
+                gram_kernel<true><<<grid, 256, 0, st>>>(Ab, lda, kai, Bb, ldb, kbj, (int)n, (int)rows, Cb, ldc);
+            else
+                gram_kernel<false><<<grid, 256, 0, st>>>(Ab, lda, kai, Bb, ldb, kbj, (int)n, (int)rows, Cb, ldc);
             CUDA_OK(cudaGetLastError());
         }
     return QD_OK;
+}
+
+// C (ka x kb) = A^H B over n rows.
+extern "C" int qd_gram_dev(int64_t n, const void *A, int64_t lda, int ka, const void *B, int64_t ldb, int kb, void *C,
+                           int ldc, void *stream) {
+    return qd_gram_ex_dev(n, A, lda, ka, B, ldb, kb, C, ldc, 1, stream);
 }
 
 // Y = Z C + beta Y (Z n x k, C k x k2 on the device with leading dimension ldc).

@@ -2,11 +2,15 @@
 and print the per-stage times: the command that the committed ncu summaries
 under profiles/ were captured from.
 
-    python -m qudos_b200.profile_solve [--mg 7] [--prec mixed|fp64] [--solves 1]
+    python -m qudos_b200.profile_solve [--mg 7] [--prec mixed|fp64] [--solves 1] [--post]
 
 One solve = H assembly (FP64, lower triangle) + the windowed eigensolve on
 the device.  With QD_PROFILE=1 in the environment the dense->band reduction
-is also broken down into its steps.
+is also broken down into its steps.  --post then runs, on the last solve's
+states, the stages that follow it in the reference: Coulomb matrix elements
+(CME = 4, Coulomb cell = electronic cell), momentum matrix elements,
+envelopes on a [001] line scan of 300 points, and the gradients with
+respect to the upper dot's height and the In fraction.
 """
 
 import argparse
@@ -29,9 +33,10 @@ def main(argv=None):
     ap.add_argument("--mg", type=int, default=7)
     ap.add_argument("--prec", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--solves", type=int, default=1)
+    ap.add_argument("--post", action="store_true")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
-        configs.write_deck(d, *configs.molecule_15(mg=a.mg))
+        configs.write_deck(d, *configs.molecule_15(mg=a.mg, cme=4 if a.post else 0))
         pr = q.Problem(d)
         pr.build_tables()
     n, lo, hi = pr.n_h, pr.lo, pr.hi
@@ -52,6 +57,27 @@ def main(argv=None):
         if os.environ.get("QD_PROFILE", "0") not in ("", "0"):
             pf = L.stage1_profile()
             print("    band reduction steps (ms): " + ", ".join("%s %.1f" % (k, v) for k, v in zip(STEPS, pf)))
+    if a.post:
+        import numpy as np
+        w = np.empty(m)
+        v = np.empty((n, m), dtype=np.complex128, order="F")
+        W.download(w)
+        Z.download(v)
+        H.free()
+        nv, nc = 2 * pr.n_vb, 2 * pr.n_cb
+        t0 = time.perf_counter()
+        pr.coulomb(v, nv, nc, 1)
+        t1 = time.perf_counter()
+        pr.momentum(v, nv, nc)
+        t2 = time.perf_counter()
+        geo = pr.geometry(pr.n_shape)[0]
+        z = np.linspace(-0.5 * geo["L3"], 0.5 * geo["L3"], 300)
+        pr.envelopes(v, np.zeros(300), np.zeros(300), z)
+        t3 = time.perf_counter()
+        pr.gradients(v[:, :8], [(L.QD_GRAD_LENGTH, 2, 3), (L.QD_GRAD_COMPOSITION, 2, 0)])
+        t4 = time.perf_counter()
+        print("post (ms wall): coulomb %.1f, momentum %.1f, envelopes %.1f, gradients %.1f" %
+              ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3, (t4 - t3) * 1e3))
     sys.stdout.flush()
 
 
