@@ -300,6 +300,11 @@ def run_gpu(args, ws, rank, local):
     H.free()
     # e2e through the reference-named C-ABI with host buffers (eigenstates)
     e2e_ms, h2d, d2h = e2e_reference_call(pr, args, L)
+    # the batched sweep of 64 generated dots (mixed 2744/5832/10648 sizes)
+    batch = None
+    if not args.no_batch:
+        from qudos_b200 import batch as qbatch
+        batch = qbatch.measure(64, 8, 0)
     cpu = None
     if rank == 0 and not args.no_cpu:
         cms, pexp, (t7, n7, t9, n9) = cpu_estimate()
@@ -351,6 +356,7 @@ def run_gpu(args, ws, rank, local):
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "batch_c5": batch,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -387,6 +393,7 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--mg", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
