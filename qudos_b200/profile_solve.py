@@ -1,16 +1,17 @@
-"""Run a few solves of the two-lens molecule deck (qudos_b200.configs.molecule_15)
-and print the per-stage times: the command that the committed ncu summaries
-under profiles/ were captured from.
+"""Run a few solves of one of the measured decks (qudos_b200.configs:
+molecule_15 by default, lens_7, pyramid_11) and print the per-stage times:
+the command that the committed ncu summaries under profiles/ were captured
+from.
 
-    python -m qudos_b200.profile_solve [--mg 7] [--prec mixed|fp64] [--solves 1] [--post]
+    python -m qudos_b200.profile_solve [--deck molecule_15] [--mg 7] [--prec mixed|fp64] [--solves 1] [--post]
 
 One solve = H assembly (FP64, lower triangle) + the windowed eigensolve on
 the device.  With QD_PROFILE=1 in the environment the dense->band reduction
 is also broken down into its steps.  --post then runs, on the last solve's
 states, the stages that follow it in the reference: Coulomb matrix elements
 (CME = 4, Coulomb cell = electronic cell), momentum matrix elements,
-envelopes on a [001] line scan of 300 points, and the gradients with
-respect to the upper dot's height and the In fraction.
+envelopes on a [001] line scan of 300 points, and the gradients of the
+lowest 8 states with respect to the (upper) dot's height and composition.
 """
 
 import argparse
@@ -34,9 +35,16 @@ def main(argv=None):
     ap.add_argument("--prec", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--solves", type=int, default=1)
     ap.add_argument("--post", action="store_true")
+    ap.add_argument("--deck", choices=["molecule_15", "lens_7", "pyramid_11"], default="molecule_15")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
-        configs.write_deck(d, *configs.molecule_15(mg=a.mg, cme=4 if a.post else 0))
+        if a.deck == "molecule_15":
+            deck = configs.molecule_15(mg=a.mg, cme=4 if a.post else 0)
+        elif a.deck == "lens_7":
+            deck = configs.lens_7(mg=a.mg)
+        else:
+            deck = configs.pyramid_11(mg=a.mg, cme=4 if a.post else 1)
+        configs.write_deck(d, *deck)
         pr = q.Problem(d)
         pr.build_tables()
     n, lo, hi = pr.n_h, pr.lo, pr.hi
@@ -52,7 +60,7 @@ def main(argv=None):
         L.check(L.lib.qd_device_synchronize())
         t = (time.perf_counter() - t0) * 1e3
         st = L.last_timings()
-        print("solve %d (%s, N_H = %d): %.1f ms wall; " % (s, a.prec, n, t) +
+        print("solve %d (%s %s, N_H = %d): %.1f ms wall; " % (s, a.deck, a.prec, n, t) +
               ", ".join("%s %.1f" % (k, v) for k, v in zip(STAGES[1:], st[1:7])))
         if os.environ.get("QD_PROFILE", "0") not in ("", "0"):
             pf = L.stage1_profile()
@@ -74,7 +82,8 @@ def main(argv=None):
         z = np.linspace(-0.5 * geo["L3"], 0.5 * geo["L3"], 300)
         pr.envelopes(v, np.zeros(300), np.zeros(300), z)
         t3 = time.perf_counter()
-        pr.gradients(v[:, :8], [(L.QD_GRAD_LENGTH, 2, 3), (L.QD_GRAD_COMPOSITION, 2, 0)])
+        dot, height = {"molecule_15": (2, 3), "lens_7": (1, 3), "pyramid_11": (1, 4)}[a.deck]
+        pr.gradients(v[:, :8], [(L.QD_GRAD_LENGTH, dot, height), (L.QD_GRAD_COMPOSITION, dot, 0)])
         t4 = time.perf_counter()
         print("post (ms wall): coulomb %.1f, momentum %.1f, envelopes %.1f, gradients %.1f" %
               ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3, (t4 - t3) * 1e3))
