@@ -477,11 +477,16 @@ extern "C" int qd_eigh_window(int64_t n, void *H, int64_t ld, int lo, int hi, in
     double bnorm;
     memcpy(&bnorm, &bm_bits, sizeof(double));
     bnorm *= (double)(2 * b + 1);
-    // groups of numerically degenerate eigenvalues share one LU factorisation
+    // Numerically degenerate eigenvalues (within 1e-10 of the band's norm: the
+    // Kramers pairs, and any accidental degeneracy on top of them) form one
+    // group of up to 64: one block factorises the band once at the group's
+    // shift and orthogonalises the group's vectors, which span the degenerate
+    // subspace.  Distinct eigenvalues keep their own shifts; two inverse
+    // iterations leave an overlap of about eps |B| / gap between them.
     std::vector<int> gs, gz;
     double tol_deg = 1e-10 * (bnorm > 1.0 ? bnorm : 1.0);
     for (int i = 0; i < k; i++) {
-        if (i > 0 && fabs(lam_h[i] - lam_h[i - 1]) <= tol_deg && gz.back() < 8) gz.back()++;
+        if (i > 0 && fabs(lam_h[i] - lam_h[i - 1]) <= tol_deg && gz.back() < 64) gz.back()++;
         else { gs.push_back(i); gz.push_back(1); }
     }
     int ng = (int)gs.size();
