@@ -1,9 +1,9 @@
 """Degenerate clusters larger than the inverse-iteration block's eight warps
 (GPU): a Hermitian matrix with a 12-fold degenerate eigenvalue inside the
-window (random unitary eigenbasis).  The FP64 and mixed solves must return
-the 12 eigenvalues within 1e-10 of the exact ones, vectors orthonormal to
-1e-10 and spanning the degenerate subspace (largest principal angle to it
-below 1e-8 for FP64)."""
+window (random unitary eigenbasis).  The FP64 (mixed) solve must return the
+window's eigenvalues within 1e-10 (1e-8) of the exact ones, vectors
+orthonormal to 1e-10, and the 12 cluster vectors spanning the degenerate
+subspace (largest principal angle below 1e-8, mixed 1e-4)."""
 
 import numpy as np
 import pytest
@@ -40,7 +40,7 @@ def test_twelve_fold_degenerate_cluster(prec):
     wg = w.download(np.empty(m))
     v = Z.download(np.empty((n, m), dtype=np.complex128, order="F"))
     ref = lam[lo:hi + 1]
-    assert np.abs(wg - ref).max() < 1e-10
+    assert np.abs(wg - ref).max() < (1e-10 if prec == q.QD_PREC_FP64 else 1e-8)
     assert np.abs(v.conj().T @ v - np.eye(m)).max() < 1e-10
     ang = sla.subspace_angles(v[:, 4:16], Q[:, lo + 4:lo + 16])
     assert ang.max() < (1e-8 if prec == q.QD_PREC_FP64 else 1e-4)
