@@ -92,6 +92,7 @@ struct eigenstate {
 /* Weak definitions live in the library.                                      */
 /* ------------------------------------------------------------------------- */
 extern int N_shape, isotropic, softening, include_strain, include_piezo, include_CME, PACKED;
+extern double sigma_softening; /* 8_band.h:90; read by coulomb_matrix_elements for commensurate cells */
 extern int myid, nprocs;
 extern int64_t N_H, na_rows, na_cols, na_rowsz, na_colsz, np_rows, np_cols, my_prow, my_pcol,
     block_size;
@@ -130,11 +131,12 @@ void eigenstates(int N_shape, int *N_states, struct vector F, struct wave_vector
  * (1: the Fourier-space integrals only; 2: plus the Madelung monopole term;
  * 3: plus dipole; 4: plus quadrupole, coulomb_matrix_elements.c:250-557), a
  * free Coulomb cell (coulomb_region_type 0) equal to or larger than the
- * electronic-structure cell, with coulomb_basis.N_G* plane waves per axis.
- * The real-space Madelung sum follows the reference's split over the
- * `nprocs` global.  Commensurate cells (coulomb_region_type 1) print an error
- * and exit.  CME arrays are allocated by the caller with the sizes of
- * 8_band_main.c:1752-1775. */
+ * electronic-structure cell, or a commensurate one (coulomb_region_type 1,
+ * supercell[0].CL* = RCL* L*; with `softening` set, the cell's cuboid is
+ * softened by `sigma_softening` as in B_coulomb_supercell_fft.c), with
+ * coulomb_basis.N_G* plane waves per axis.  The real-space Madelung sum
+ * follows the reference's split over the `nprocs` global.  CME arrays are
+ * allocated by the caller with the sizes of 8_band_main.c:1752-1775. */
 void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coulomb_basis,
                              struct supercell_geometry *supercell,
                              struct material_params *parameters, int *N_states,
@@ -244,8 +246,9 @@ int qd_eigh_window_dev(int64_t n, void *H_dev, int64_t ld, int lo, int hi, int p
  * eigensolve; eigval (M) and eigvec (N_H x M) in host memory. */
 int qd_problem_solve(qd_problem *pr, int prec, double *eigval, qd_complex128 *eigvec);
 
-/* Coulomb matrix elements (coulomb_matrix_elements.c:24, free Coulomb-cell
- * lengths, the problem's CME setting 1..4) for n_vb_states + n_cb_states
+/* Coulomb matrix elements (coulomb_matrix_elements.c:24, free or
+ * commensurate Coulomb cells as the deck's Coulomb_supercell_type says, the
+ * problem's CME setting 1..4) for n_vb_states + n_cb_states
  * states (eigvec_host: N_H x M_c, VB states first, as eigenstates orders
  * them) into the reference's four arrays (sizes of 8_band_main.c:1752-1755;
  * elements outside the reference's computed set are zero).  The real-space

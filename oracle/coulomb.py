@@ -10,6 +10,9 @@ Follows the reference's ``coulomb_matrix_elements`` path
 * ``coulomb_supercell``   B on the Coulomb-cell grid, free cell lengths
                           (B_coulomb_supercell.c:23-139; identity when the
                           cells and plane-wave counts agree);
+* ``coulomb_supercell_commensurate``  the same for Coulomb cells of RCL times
+                          the electronic cell (B_coulomb_supercell_fft.c:23-100,
+                          characteristic_function_coulomb_supercell.c:24-72);
 * ``wavevector_prefactor``w(G) = e^2/eps0 / (V_C G^2 n_r^2), w(0) = 0
                           (coulomb_matrix_elements.c:370-401);
 * ``corrections``         CME >= 2: Madelung constant, dipole and quadrupole
@@ -110,6 +113,35 @@ def coulomb_supercell(B, basis, cbasis, L, CL):
         out = (((inv_vol * Bt) * L[0]) * L[1]) * L[2]
         return out.reshape(P, -1)
     out = np.einsum("xa,yb,zc,pabc->pxyz", W[0], W[1], W[2], Bt) * inv_vol
+    return out.reshape(P, -1)
+
+
+def coulomb_supercell_commensurate(B, basis, cbasis, geo, softening=0, sigma=0.0):
+    """B on the Coulomb-cell grid for Coulomb_supercell_type 1, CL = RCL L
+    (B_convolutions.c:170-300 and B_coulomb_supercell_fft.c:23-100): B is
+    placed on every RCL-th point of a grid of NC_T + 2 RCL (N_T / 2) points per
+    axis, convolved (forward FFTs, product, backward FFT with scale 1/size)
+    with the electronic cell's cuboid (shape record 0) tabulated on the Coulomb
+    grid with the Coulomb-cell normalisation, and the central NC_T block is
+    scaled by CL1 CL2 CL3 / (L1 L2 L3).  ``B`` holds the pair functions on the
+    (2N-1)^3 grid as returned by ``b_functions``."""
+    g0 = geo[0]
+    RC = (g0["RCL1"], g0["RCL2"], g0["RCL3"])
+    NT = basis["N_T"]
+    NCT = cbasis["N_T"]
+    S = tuple(NCT[a] + 2 * RC[a] * (NT[a] // 2) for a in range(3))
+    chi = shapes.chi_table(cbasis, geo, 0, 3, softening, sigma)
+    X = np.zeros(S, dtype=np.complex128)
+    X[:NCT[0], :NCT[1], :NCT[2]] = chi
+    X = np.fft.fftn(X)
+    P = B.shape[0]
+    up = np.zeros((P,) + S, dtype=np.complex128)
+    up[:, : RC[0] * NT[0]: RC[0], : RC[1] * NT[1]: RC[1], : RC[2] * NT[2]: RC[2]] = B.reshape((P,) + NT)
+    axes = (-3, -2, -1)
+    conv = np.fft.ifftn(np.fft.fftn(up, axes=axes) * X[None], axes=axes)
+    o = [S[a] // 2 - NCT[a] // 2 for a in range(3)]
+    scale = (g0["CL1"] * g0["CL2"] * g0["CL3"]) / (g0["L1"] * g0["L2"] * g0["L3"])
+    out = scale * conv[:, o[0]: o[0] + NCT[0], o[1]: o[1] + NCT[1], o[2]: o[2] + NCT[2]]
     return out.reshape(P, -1)
 
 
@@ -304,15 +336,20 @@ def integrals(B, Brw, nv, nc, nr, CL, corr, cme):
     return {"hh": hh, "ee": ee, "eh_direct": ehd, "eh_exchange": ehx}
 
 
-def coulomb_matrix_elements(basis, geo, params, vecs, nv, nc, NC, cme=1, ranks=4):
-    """All four arrays for states vecs (N_H x (nv + nc), VB states first)."""
+def coulomb_matrix_elements(basis, geo, params, vecs, nv, nc, NC, cme=1, ranks=4, cell_type=0, softening=0,
+                            sigma=0.0):
+    """All four arrays for states vecs (N_H x (nv + nc), VB states first).
+    ``cell_type`` is Coulomb_supercell_type (0 free lengths, 1 RCL multiples)."""
     g0 = geo[0]
     L = (g0["L1"], g0["L2"], g0["L3"])
     CL = (g0["CL1"], g0["CL2"], g0["CL3"])
     cbasis = shapes.make_basis(NC, CL)
     nr = params[0]["nr"]
     B = b_functions(vecs, basis["N"])
-    Bc = coulomb_supercell(B, basis, cbasis, L, CL)
+    if cell_type == 1:
+        Bc = coulomb_supercell_commensurate(B, basis, cbasis, geo, softening, sigma)
+    else:
+        Bc = coulomb_supercell(B, basis, cbasis, L, CL)
     w = wavevector_prefactor(cbasis, CL, nr)
     Brw = Bc[:, ::-1] * w[None, :]
     corr = corrections(Bc, cbasis, CL, nv + nc, cme, ranks)

@@ -31,8 +31,8 @@ def prepare(p, geo):
     include_strain = p["Strain"]
     pr.tables = hamiltonian.Tables([None] * ns)
     if include_strain == 1:
-        if pr.strain_type != 0:
-            raise NotImplementedError("commensurate strain-cell downsampling is not in the oracle")
+        if pr.strain_type == 1 and strain.strain_grid_too_small(p, geo):
+            raise ValueError("M_S is too small for the commensurate strain cell")
         pr.strain_basis = shapes.make_basis((p["N_S_Gx"], p["N_S_Gy"], p["N_S_Gz"]),
                                             (g0["SL1"], g0["SL2"], g0["SL3"]), K)
         chi_s = [None] + [shapes.chi_table(pr.strain_basis, geo, s, 1, soft, sig) for s in range(1, ns)]
@@ -43,11 +43,17 @@ def prepare(p, geo):
         else:
             chi_es = [None] + [shapes.chi_table(pr.basis, geo, s, 0, soft, sig) for s in range(1, ns)]
         eps_s = strain.strain_region(pr.strain_basis, geo, pr.params, chi_s, p["Isotropic"])
-        eps = {c: strain.downsample(eps_s[c], pr.basis, pr.strain_basis, geo) for c in strain.COMPONENTS}
+        if pr.strain_type == 1:  # main:587-600, 634-646
+            def down(t):
+                return strain.downsample_commensurate(t, pr.basis, pr.strain_basis, geo, soft, sig)
+        else:
+            def down(t):
+                return strain.downsample(t, pr.basis, pr.strain_basis, geo)
+        eps = {c: down(eps_s[c]) for c in strain.COMPONENTS}
         phi = None
         if p["Piezo"] != 0:
             phi_s = strain.piezo_region(pr.strain_basis, geo, pr.params, chi_s, eps_s, p["Piezo"])
-            phi = strain.downsample(phi_s, pr.basis, pr.strain_basis, geo)
+            phi = down(phi_s)
         conv = strain.convolutions(chi_es, eps, ns)
         pr.tables = hamiltonian.Tables(chi_es, eps, conv, phi)
         pr.chi_strain, pr.eps_strain = chi_s, eps_s

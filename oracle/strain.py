@@ -6,6 +6,9 @@ Follows (test infrastructure):
   * ``piezo_region_reciprocal_space.c:23-787`` + ``piezo_fourier_coefficient.c:24-132``,
   * ``strain_reciprocal_space.c:23-230`` / ``piezo_reciprocal_space.c:23-186``
     (free-length downsampling; the identity copy when the cells coincide),
+  * ``strain_reciprocal_space_fft.c:23-362`` / ``piezo_reciprocal_space_fft.c``
+    (commensurate strain cells SL = RL L: FFT convolution with the electronic
+    cell's box, sampled at every RL-th strain-cell wave vector),
   * ``convolutions.c:24-411``.
 
 Tables are numpy arrays of shape (N_xT, N_yT, N_zT) (flat index
@@ -167,6 +170,39 @@ def downsample(table_s, basis, strain_basis, geo):
     My = _axis_factor(strain_basis["G"][1], basis["G"][1], L[1], same[1])
     Mz = _axis_factor(strain_basis["G"][2], basis["G"][2], L[2], same[2])
     return inv_v * np.einsum("abc,ai,bj,ck->ijk", table_s, Mx, My, Mz)
+
+
+def downsample_commensurate(table_s, basis, strain_basis, geo, softening=0, sigma=0.0):
+    """Strain-cell table -> electronic-structure cell for commensurate lengths
+    (Strain_supercell_type 1, strain_reciprocal_space_fft.c:23-362 and
+    piezo_reciprocal_space_fft.c, the same steps for phi): chi_0, the
+    electronic cell's cuboid (shape record 0, normalised by the electronic cell
+    volume, softened like every shape) on the strain grid, and the table are
+    zero-padded to (2 N_ST - 1)^3, multiplied after a forward FFT and
+    transformed back (backward scale 1/size); the electronic-cell coefficient of
+    index i is the element RL i + N_ST - 1 - RL (N_T / 2) of the result along
+    each axis."""
+    from . import shapes
+    chi0 = shapes.chi_table(strain_basis, geo, 0, 2, softening, sigma)
+    conv = np.fft.ifftn(np.fft.fftn(pad(chi0)) * np.fft.fftn(pad(table_s)))
+    g0 = geo[0]
+    RL = (g0["RL1"], g0["RL2"], g0["RL3"])
+    nS = table_s.shape
+    nE = basis["N_T"]
+    idx = [RL[a] * np.arange(nE[a]) + nS[a] - 1 - RL[a] * (nE[a] // 2) for a in range(3)]
+    return conv[np.ix_(*idx)]
+
+
+def strain_grid_too_small(p, geo):
+    """8_band_main.c:159-192: with commensurate strain cells, M_S must reach
+    about M RL / 2 along every axis.  Returns the axes that fail."""
+    g0 = geo[0]
+    bad = []
+    for a, ax in enumerate("xyz"):
+        n, ns, rl = p["N_G" + ax], p["N_S_G" + ax], g0["RL%d" % (a + 1)]
+        if ns // 2 < (n // 2) * rl // 2 + ((n // 2) % 2) * (rl % 2):
+            bad.append(ax)
+    return bad
 
 
 def convolutions(chi_es, strain_es, n_shape):

@@ -1,5 +1,5 @@
 // Coulomb matrix elements on the GPU (code/source/8_band/coulomb_matrix_elements.c:24-627
-// and the routines it calls, for free Coulomb-cell lengths, CME = 1..4).
+// and the routines it calls, for free and commensurate Coulomb cells, CME = 1..4).
 //
 //   1. padded envelopes a_sb and conjugate-reversed copies per state and band
 //      on the (2Nx-1)(2Ny-1)(2Nz-1) grid (state_redistribution.c:45-66);
@@ -10,7 +10,13 @@
 //      reference transforms back per band and then adds; the transform is
 //      linear, so summing first is the same B_ij, B_convolutions.c:332-390);
 //   4. B on the Coulomb-cell grid: a scaled copy when the cells agree, else
-//      separable sinc weights per axis (B_coulomb_supercell.c:23-139);
+//      separable sinc weights per axis (B_coulomb_supercell.c:23-139).  For
+//      commensurate cells (CL = RCL L) the reference upsamples B onto every
+//      RCL-th point and convolves it by FFTs with the electronic cell's cuboid
+//      on the Coulomb grid (B_coulomb_supercell_fft.c:23-100); that linear
+//      convolution is the same separable sum with the cut-off |GC - G| <=
+//      max GC, times the cuboid's softening factor when softening is on;
+//      tests check it against the FFT form;
 //   5. w(G) times the reversed B (coulomb_matrix_elements.c:370-401, 498-503);
 //   6. every pair-pair contraction at once as two reductions over the grid
 //      (sum Brw_q B_p and sum conj(Brw_q) B_p), and the dipole/quadrupole
@@ -148,6 +154,8 @@ struct QdCoulombSpec {
     double nr;     // refractive index of the matrix material
     int cme;       // include_CME (1..4)
     int ranks;     // ranks whose blocks the real-space Madelung sum covers
+    int commensurate;  // Coulomb_supercell_type 1: CL = RCL L
+    double soft_sigma; // Gaussian softening of the cell's cuboid (commensurate cells; 0 = none)
 };
 
 namespace {
@@ -364,6 +372,7 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
                     if (fabs(d) < QD_EPS) v = sp->L[a];
                     else if (fabs(d) > Gc[szC[a] - 1] + QD_EPS) v = 0.0;
                     else v = 2 * sin(d * sp->L[a] / 2) / d;
+                    if (sp->soft_sigma != 0.0) v *= exp(-0.5 * sp->soft_sigma * sp->soft_sigma * d * d);
                     Wh[a * 128 * 128 + c * sz3[a] + g] = v;
                 }
         }
@@ -484,9 +493,11 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
 }
 
 static int spec_from_problem(const qd_problem *pr, int ranks, QdCoulombSpec *sp) {
-    if (pr->p.coulomb_type != 0)
-        return qd_set_error(QD_ERR_UNSUPPORTED, "Coulomb_supercell_type 1 (commensurate cells) is not supported");
     const struct supercell_geometry *g = &pr->geo[0];
+    if (pr->p.coulomb_type == 1 && (g->RCL1 < 1 || g->RCL2 < 1 || g->RCL3 < 1))
+        return qd_set_error(QD_ERR_INPUT, "relative Coulomb lengths must be >= 1");
+    sp->commensurate = pr->p.coulomb_type == 1;
+    sp->soft_sigma = (sp->commensurate && pr->p.softening != 0) ? pr->p.sigma : 0.0;
     for (int a = 0; a < 3; a++) {
         sp->N[a] = pr->p.N[a];
         sp->NC[a] = pr->p.NC[a];
@@ -530,9 +541,9 @@ extern "C" void coulomb_matrix_elements(struct wave_vectors basis, struct wave_v
                                         struct eigenstate *eigenstate_cb, struct coulomb_matrix_element CME,
                                         int coulomb_region_type) {
     int rc = QD_OK;
-    if (coulomb_region_type != 0)
-        rc = qd_set_error(QD_ERR_UNSUPPORTED, "Coulomb_supercell_type 1 (commensurate cells) is not supported");
     QdCoulombSpec sp;
+    sp.commensurate = coulomb_region_type == 1;
+    sp.soft_sigma = (sp.commensurate && softening != 0) ? sigma_softening : 0.0;
     sp.N[0] = basis.N_Gx;
     sp.N[1] = basis.N_Gy;
     sp.N[2] = basis.N_Gz;

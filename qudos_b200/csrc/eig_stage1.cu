@@ -747,11 +747,25 @@ extern "C" int qd_stage1_backtransform(const void *A, int64_t n, int64_t lda, in
     return backtransform<cuDoubleComplex>((const cuDoubleComplex *)A, n, lda, b, w, (cuDoubleComplex *)Z, ldz, mz, st);
 }
 
+// Uniform values in [-1, 1) from a 64-bit integer hash of the index
+// (splitmix64 finaliser), so that the peak GEMM runs on dense nonzero data.
+__global__ void fill_uniform_kernel(double *d, float *f, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long z = i + 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        const double v = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+        if (d) d[i] = v;
+        if (f) f[i] = (float)v;
+    }
+}
+
 // Throughput of a plain cuBLAS GEMM (the denominators of the roofline
 // fractions that the measured-peak file does not hold): kind 0 DGEMM (FP64),
-// 1 SGEMM with TF32 tensor-core inputs, 2 ZGEMM.  n x n x n, `reps` timed
-// back-to-back launches after one warm-up; returns TFLOP/s (2 n^3 per real
-// GEMM, 8 n^3 per complex GEMM).
+// 1 SGEMM with TF32 tensor-core inputs, 2 ZGEMM.  n x n x n on operands
+// filled with uniform random values, `reps` timed back-to-back launches after
+// one warm-up; returns TFLOP/s (2 n^3 per real GEMM, 8 n^3 per complex GEMM).
 extern "C" int qd_gemm_peak(int kind, int n, int reps, double *tflops) {
     if (kind < 0 || kind > 2 || n < 64 || reps < 1) return qd_set_error(QD_ERR_ARG, "qd_gemm_peak: bad arguments");
     cublasHandle_t h = qd_cublas();
@@ -766,8 +780,11 @@ extern "C" int qd_gemm_peak(int kind, int n, int reps, double *tflops) {
         cudaGetLastError();
         return qd_set_error(QD_ERR_NOMEM, "qd_gemm_peak");
     }
-    cudaMemset(A, 0, bytes);
-    cudaMemset(B, 0, bytes);
+    const size_t nel = bytes / (kind == 1 ? 4 : 8);
+    fill_uniform_kernel<<<148 * 8, 256, 0, cudaStreamPerThread>>>(kind == 1 ? nullptr : (double *)A,
+                                                                   kind == 1 ? (float *)A : nullptr, nel);
+    fill_uniform_kernel<<<148 * 8, 256, 0, cudaStreamPerThread>>>(kind == 1 ? nullptr : (double *)B,
+                                                                   kind == 1 ? (float *)B : nullptr, nel);
     BLAS_OK(cublasSetStream(h, cudaStreamPerThread));
     const double d1 = 1.0, d0 = 0.0;
     const float f1 = 1.0f, f0 = 0.0f;
@@ -786,9 +803,9 @@ extern "C" int qd_gemm_peak(int kind, int n, int reps, double *tflops) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cublasStatus_t st = run();
-    cudaEventRecord(e0, 0);
+    cudaEventRecord(e0, cudaStreamPerThread);
     for (int r = 0; r < reps && st == CUBLAS_STATUS_SUCCESS; r++) st = run();
-    cudaEventRecord(e1, 0);
+    cudaEventRecord(e1, cudaStreamPerThread);
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);

@@ -23,6 +23,7 @@
 QD_WEAK int N_shape = 0;
 QD_WEAK int isotropic = 0;
 QD_WEAK int softening = 0;
+QD_WEAK double sigma_softening = 0.0;
 QD_WEAK int include_strain = 0;
 QD_WEAK int include_piezo = 0;
 QD_WEAK int include_CME = 0;

@@ -490,6 +490,67 @@ __global__ void downsample_kernel(const double2 *in, int64_t sin_, double2 *out,
     out[b * sout + t] = acc.d2();
 }
 
+// Commensurate strain cells, SL = RL L (strain_reciprocal_space_fft.c:23-362,
+// piezo_reciprocal_space_fft.c): the reference convolves the strain-cell table
+// with chi_0, the electronic cell's cuboid (shape record 0) on the strain grid,
+// by zero-padded FFTs and keeps every RL-th point about the centre.  chi_0 is a
+// product over axes (L sinc(G L / 2), softened like every shape, times
+// 1/(L1 L2 L3)), so the same linear convolution is the separable sum
+//   T_es(e) = 1/(L1 L2 L3) sum_s prod_a w_a(e_a, s_a) T_s(s),
+//   w_a(e, s) = L_a sinc(GS_a[q] L_a / 2) exp(-sigma^2 GS_a[q]^2 / 2),
+//   q = RL_a (e - h_a) - (s - hs_a) + hs_a  (h, hs: centre indices),
+// with w = 0 where q leaves the strain grid (the support of the padded chi_0).
+// Weights of one axis, row-major n_e x n_s.
+__global__ void comm_weights_kernel(const double *GS, int ns, int ne, int RL, double L, int softening, double sigma,
+                                    double *W) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne * ns) return;
+    const int e = t / ns, s = t % ns, hs = ns / 2, h = ne / 2;
+    const int q = RL * (e - h) - (s - hs) + hs;
+    double v = 0.0;
+    if (q >= 0 && q < ns) {
+        const double g = GS[q];
+        v = L * sinc_pi((0.5 * g * L) / M_PI);
+        if (softening != 0) v *= exp(-0.5 * sigma * sigma * g * g);
+    }
+    W[t] = v;
+}
+
+// One axis of a separable linear map on nb complex arrays [x][y][z] of extents
+// (d0, d1, d2): along `axis` its d[axis] points become n_out points,
+// out = scale * W in, W row-major (n_out x d[axis]).
+__global__ void sep_axis_kernel(const double2 *in, int64_t sin_, int d0, int d1, int d2, int axis, int n_out,
+                                const double *W, double scale, int nb, double2 *out, int64_t sout) {
+    const int n_in = axis == 0 ? d0 : axis == 1 ? d1 : d2;
+    const int o0 = axis == 0 ? n_out : d0, o1 = axis == 1 ? n_out : d1, o2 = axis == 2 ? n_out : d2;
+    const int64_t n = (int64_t)o0 * o1 * o2;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (t >= n || b >= nb) return;
+    int i0 = (int)(t / ((int64_t)o1 * o2)), i1 = (int)((t / o2) % o1), i2 = (int)(t % o2);
+    int e;
+    int64_t stride;
+    if (axis == 0) {
+        e = i0; i0 = 0; stride = (int64_t)d1 * d2;
+    } else if (axis == 1) {
+        e = i1; i1 = 0; stride = d2;
+    } else {
+        e = i2; i2 = 0; stride = 1;
+    }
+    const double2 *src = in + b * sin_ + ((int64_t)i0 * d1 + i1) * d2 + i2;
+    const double *w = W + (int64_t)e * n_in;
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < n_in; k++) {
+        const double wk = w[k];
+        if (wk != 0.0) {
+            const double2 v = src[k * stride];
+            re += wk * v.x;
+            im += wk * v.y;
+        }
+    }
+    out[b * sout + t] = make_double2(scale * re, scale * im);
+}
+
 // hydrostatic / biaxial combinations of the six chi (*) eps tables (convolutions.c:313-314)
 __global__ void hydro_biax_kernel(double2 *conv8, int64_t n) {
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -646,8 +707,17 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
     }
     if (P.strain && P.elastic_const != 0)
         return qd_set_error(QD_ERR_UNSUPPORTED, "position-dependent elastic constants (Elastic_const: 1)");
-    if (P.strain && pr->p.strain_type != 0)
-        return qd_set_error(QD_ERR_UNSUPPORTED, "commensurate strain-cell downsampling with RL > 1");
+    if (P.strain && pr->p.strain_type == 1) {
+        // 8_band_main.c:159-192: the strain grid must resolve every RL-th wave vector
+        const int rl[3] = {pr->geo[0].RL1, pr->geo[0].RL2, pr->geo[0].RL3};
+        for (int a = 0; a < 3; a++) {
+            if (rl[a] < 1) return qd_set_error(QD_ERR_INPUT, "relative strain length %d must be >= 1", a + 1);
+            const int n2 = P.N[a] / 2;
+            if (P.NS[a] / 2 < n2 * rl[a] / 2 + (n2 % 2) * (rl[a] % 2))
+                return qd_set_error(QD_ERR_INPUT, "M_S_G%c is too small for the relative strain length %d",
+                                    "xyz"[a], rl[a]);
+        }
+    }
     int64_t nT = pr->nT, nTS = pr->nTS;
     // device copies of geometry, materials, grids
     RC(dalloc(&pr->d_geo, sizeof(geo_t) * ns));
@@ -757,26 +827,61 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
                                                                      P.sigma, chi);
             CK(cudaGetLastError());
         }
-        // downsample strain and phi (free lengths; identity when the cells coincide)
+        // downsample strain and phi (free lengths, identity when the cells coincide; or commensurate lengths)
         RC(dalloc(&eps, sizeof(double2) * nT * 6));
         RC(dalloc(&phi, sizeof(double2) * nT));
         CK(cudaMemset(phi, 0, sizeof(double2) * nT));
         const geo_t &g0 = pr->geo[0];
-        int same[3];
-        for (int a = 0; a < 3; a++) {
-            double L = a == 0 ? g0.L1 : a == 1 ? g0.L2 : g0.L3, SL = a == 0 ? g0.SL1 : a == 1 ? g0.SL2 : g0.SL3;
-            same[a] = P.N[a] == P.NS[a] && L == SL;
-        }
-        downsample_kernel<<<dim3(nblk(nT, 128), 6), 128, 0, st>>>(
-            eps_s, nTS, eps, nT, 6, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0], pr->NT[1], pr->NT[2], pr->d_GS[0],
-            pr->d_GS[1], pr->d_GS[2], pr->NTS[0], pr->NTS[1], pr->NTS[2], g0.L1, g0.L2, g0.L3, same[0], same[1],
-            same[2]);
-        if (P.piezo != 0)
-            downsample_kernel<<<dim3(nblk(nT, 128), 1), 128, 0, st>>>(
-                phi_s, nTS, phi, nT, 1, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0], pr->NT[1], pr->NT[2],
+        if (P.strain_type == 1) {
+            // commensurate cells: three separable passes (z, y, x) with the weights above
+            const int *NTS = pr->NTS, *NT = pr->NT;
+            const int rl[3] = {g0.RL1, g0.RL2, g0.RL3};
+            const double Ls[3] = {g0.L1, g0.L2, g0.L3};
+            double *W;
+            double2 *t0, *t1;
+            const int64_t woff[3] = {0, (int64_t)NT[0] * NTS[0], (int64_t)NT[0] * NTS[0] + (int64_t)NT[1] * NTS[1]};
+            const int64_t n0 = (int64_t)NTS[0] * NTS[1] * NT[2], n1 = (int64_t)NTS[0] * NT[1] * NT[2];
+            RC(dalloc(&W, sizeof(double) * (woff[2] + (int64_t)NT[2] * NTS[2])));
+            RC(dalloc(&t0, sizeof(double2) * n0 * 6));
+            RC(dalloc(&t1, sizeof(double2) * n1 * 6));
+            for (int a = 0; a < 3; a++)
+                comm_weights_kernel<<<nblk((int64_t)NT[a] * NTS[a], 128), 128, 0, st>>>(
+                    pr->d_GS[a], NTS[a], NT[a], rl[a], Ls[a], P.softening, P.sigma, W + woff[a]);
+            const double inv_v = 1.0 / (g0.L1 * g0.L2 * g0.L3);
+            for (int pass = 0; pass < 2; pass++) {
+                const int nb = pass == 0 ? 6 : 1;
+                if (pass == 1 && P.piezo == 0) break;
+                const double2 *src = pass == 0 ? eps_s : phi_s;
+                double2 *dst = pass == 0 ? eps : phi;
+                sep_axis_kernel<<<dim3(nblk(n0, 128), nb), 128, 0, st>>>(src, nTS, NTS[0], NTS[1], NTS[2], 2, NT[2],
+                                                                         W + woff[2], 1.0, nb, t0, n0);
+                sep_axis_kernel<<<dim3(nblk(n1, 128), nb), 128, 0, st>>>(t0, n0, NTS[0], NTS[1], NT[2], 1, NT[1],
+                                                                         W + woff[1], 1.0, nb, t1, n1);
+                sep_axis_kernel<<<dim3(nblk(nT, 128), nb), 128, 0, st>>>(t1, n1, NTS[0], NT[1], NT[2], 0, NT[0],
+                                                                         W + woff[0], inv_v, nb, dst, nT);
+            }
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));
+            cudaFree(W);
+            cudaFree(t0);
+            cudaFree(t1);
+        } else {
+            int same[3];
+            for (int a = 0; a < 3; a++) {
+                double L = a == 0 ? g0.L1 : a == 1 ? g0.L2 : g0.L3, SL = a == 0 ? g0.SL1 : a == 1 ? g0.SL2 : g0.SL3;
+                same[a] = P.N[a] == P.NS[a] && L == SL;
+            }
+            downsample_kernel<<<dim3(nblk(nT, 128), 6), 128, 0, st>>>(
+                eps_s, nTS, eps, nT, 6, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0], pr->NT[1], pr->NT[2],
                 pr->d_GS[0], pr->d_GS[1], pr->d_GS[2], pr->NTS[0], pr->NTS[1], pr->NTS[2], g0.L1, g0.L2, g0.L3,
                 same[0], same[1], same[2]);
-        CK(cudaGetLastError());
+            if (P.piezo != 0)
+                downsample_kernel<<<dim3(nblk(nT, 128), 1), 128, 0, st>>>(
+                    phi_s, nTS, phi, nT, 1, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0], pr->NT[1], pr->NT[2],
+                    pr->d_GS[0], pr->d_GS[1], pr->d_GS[2], pr->NTS[0], pr->NTS[1], pr->NTS[2], g0.L1, g0.L2, g0.L3,
+                    same[0], same[1], same[2]);
+            CK(cudaGetLastError());
+        }
         pr->d_eps = eps; pr->d_phi = phi;
         // convolutions chi_s (*) eps_ij (convolutions.c)
         Grid3 pg = {{2 * pr->NT[0] - 1, 2 * pr->NT[1] - 1, 2 * pr->NT[2] - 1}};

@@ -7,9 +7,10 @@ from.
 
 One solve = H assembly (FP64, lower triangle) + the windowed eigensolve on
 the device.  With QD_PROFILE=1 in the environment the dense->band reduction
-is also broken down into its steps.  --post then runs, on the last solve's
-states, the stages that follow it in the reference: Coulomb matrix elements
-(CME = 4, Coulomb cell = electronic cell), momentum matrix elements,
+is also broken down into its steps.  --post then runs twice (a first pass
+with the one-time costs and a warm one), on the last solve's states, the
+stages that follow it in the reference: Coulomb matrix elements (the deck's
+CME setting and Coulomb cell), momentum matrix elements,
 envelopes on a [001] line scan of 300 points, and the gradients of the
 lowest 8 states with respect to the (upper) dot's height and composition.
 """
@@ -73,20 +74,22 @@ def main(argv=None):
         Z.download(v)
         H.free()
         nv, nc = 2 * pr.n_vb, 2 * pr.n_cb
-        t0 = time.perf_counter()
-        pr.coulomb(v, nv, nc, 1)
-        t1 = time.perf_counter()
-        pr.momentum(v, nv, nc)
-        t2 = time.perf_counter()
         geo = pr.geometry(pr.n_shape)[0]
         z = np.linspace(-0.5 * geo["L3"], 0.5 * geo["L3"], 300)
-        pr.envelopes(v, np.zeros(300), np.zeros(300), z)
-        t3 = time.perf_counter()
         dot, height = {"molecule_15": (2, 3), "lens_7": (1, 3), "pyramid_11": (1, 4)}[a.deck]
-        pr.gradients(v[:, :8], [(L.QD_GRAD_LENGTH, dot, height), (L.QD_GRAD_COMPOSITION, dot, 0)])
-        t4 = time.perf_counter()
-        print("post (ms wall): coulomb %.1f, momentum %.1f, envelopes %.1f, gradients %.1f" %
-              ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3, (t4 - t3) * 1e3))
+        # the first pass includes one-time costs (kernel loading, pool growth); the second is warm
+        for rep in ("first", "warm"):
+            t0 = time.perf_counter()
+            pr.coulomb(v, nv, nc, 1)
+            t1 = time.perf_counter()
+            pr.momentum(v, nv, nc)
+            t2 = time.perf_counter()
+            pr.envelopes(v, np.zeros(300), np.zeros(300), z)
+            t3 = time.perf_counter()
+            pr.gradients(v[:, :8], [(L.QD_GRAD_LENGTH, dot, height), (L.QD_GRAD_COMPOSITION, dot, 0)])
+            t4 = time.perf_counter()
+            print("post, %s pass (ms wall): coulomb %.1f, momentum %.1f, envelopes %.1f, gradients %.1f" %
+                  (rep, (t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3, (t4 - t3) * 1e3))
     sys.stdout.flush()
 
 

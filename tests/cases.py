@@ -55,5 +55,20 @@ def isotropic(mg, tmp):
     return C.write_deck(os.path.join(str(tmp), "iso_%d" % mg), params, cell)
 
 
+def commensurate(mg, tmp):
+    """Commensurate strain cell (Strain_supercell_type 1, RL = 2, 2, 3 with
+    M_S = M RL) and Coulomb cell (Coulomb_supercell_type 1, RCL = 1, 2, 2);
+    truncated pyramid on a wetting layer, first + second order piezo and
+    interface softening (sigma 0.3 nm)."""
+    rl = (2, 2, 3)
+    params = C.parameters_text(N_shape=3, M_Gx=mg, M_Gy=mg, M_Gz=mg, M_S_Gx=mg * rl[0], M_S_Gy=mg * rl[1],
+                               M_S_Gz=mg * rl[2], N_VB=2, N_CB=1, Piezo=2, CME=4, Coulomb_supercell_type=1,
+                               M_C_Gx=mg, M_C_Gy=2 * mg, M_C_Gz=2 * mg, Softening=1, Sigma_softening=0.3)
+    cell = (C.supercell_record((20.0, 20.0, 14.0), strain_rel=rl, coulomb=(1, 2, 2)) +
+            C.shape_record(6, 3, 0.5, 0.0, (0.0, 0.0, -1.5), (6.0, 6.0, 3.0, 3.0)) +
+            C.shape_record(17, 3, 0.5, 0.0, (0.0, 0.0, -1.8), (2.0, 0.5)))
+    return C.write_deck(os.path.join(str(tmp), "comm_%d" % mg), params, cell)
+
+
 CASES = {"prism": prism, "lens": lens, "pyramid": pyramid, "molecule": molecule, "nostrain_k": nostrain_k,
-         "isotropic": isotropic}
+         "isotropic": isotropic, "commensurate": commensurate}

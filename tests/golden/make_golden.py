@@ -16,8 +16,9 @@ the rotation of the two states of a Kramers pair:
   ``momentum_matrix_elements.dat`` ([100], [010], [001], [110], [-110]) the sums
   of |p|^2 over the four (CB state, VB state) combinations of a CB pair and a
   VB pair;
-* ``probability_pairs.npz``: the probability densities of the line scans along
-  [100], [001] and [111] (``probability_density_{vb,cb}_<k>_<dir>.dat``, columns
+* ``probability_pairs.npz``: the probability densities of the example's line
+  scans ([100], [001], [111] for Prism_111; [100], [010], [001] for
+  Truncated_pyramid; ``probability_density_{vb,cb}_<k>_<dir>.dat``, columns
   total, SO, LH, HH, CB in nm^-3) summed over the two states of each pair.
 The tests read only these fixtures, never the reference checkout.
 """
@@ -28,7 +29,9 @@ import sys
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
 
-EXAMPLES = {"prism_111": "Prism_111"}
+# fixture directory -> (example, line scans in its golden outputs)
+EXAMPLES = {"prism_111": ("Prism_111", ("100", "001", "111")),
+            "truncated_pyramid": ("Truncated_pyramid", ("100", "010", "001"))}
 
 
 def strip_comments(text):
@@ -42,7 +45,7 @@ def strip_comments(text):
 
 def main(ref):
     here = os.path.dirname(os.path.abspath(__file__))
-    for name, ex in EXAMPLES.items():
+    for name, (ex, scans) in EXAMPLES.items():
         src = os.path.join(ref, "code", "example", ex, "Electronic_structure")
         dst = os.path.join(here, name)
         os.makedirs(dst, exist_ok=True)
@@ -70,7 +73,7 @@ def main(ref):
                        "units": "eV (|p|^2 / (HBSQM / 2))", "pair_sums": sums.tolist()}, fo, indent=1)
         # probability densities of three line scans, summed over Kramers pairs
         arrays = {}
-        for tag in ("100", "001", "111"):
+        for tag in scans:
             for band, n in (("vb", nvs), ("cb", ncs)):
                 rows = [np.loadtxt(os.path.join(ref_dir, "probability_density_%s_%d_%s.dat" % (band, k + 1, tag)))
                         for k in range(n)]

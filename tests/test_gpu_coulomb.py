@@ -4,9 +4,13 @@
   every element is populated) through qd_coulomb and the oracle, for CME 1-4,
   a Coulomb cell equal to the electronic cell and a larger free Coulomb cell
   with more plane waves; max |dV| <= 1e-11 max |V|.
-* Golden: the reference's Prism_111 example solved on the GPU (FP64), its
-  Coulomb elements with CME = 4 on 4 Madelung ranks, and the direct terms
-  between Kramers pairs against the reference's output files (10 digits).
+* Commensurate Coulomb cells (Coulomb_supercell_type 1, with softening)
+  against the oracle's FFT form of B_coulomb_supercell_fft.c.
+* Golden: the reference's Prism_111 (free Coulomb cell) and
+  Truncated_pyramid (commensurate Coulomb cell, RCL = 1, 1, 2) examples
+  solved on the GPU (FP64), their Coulomb elements with CME = 4 on 4 Madelung
+  ranks, and the direct terms between Kramers pairs against the reference's
+  output files (10 digits).
 """
 
 import json
@@ -60,9 +64,35 @@ def test_coulomb_matches_oracle(tmp_path, mg, mc, cme, cell):
         assert np.array_equal(got[k] == 0, ref[k] == 0), k
 
 
-def test_coulomb_prism_111_golden_direct_terms():
-    gold = json.load(open(os.path.join(GOLDEN, "coulomb_direct.json")))
-    prob = q.Problem(GOLDEN)
+@pytest.mark.parametrize("mg", [1, 2])
+def test_coulomb_commensurate_cells_match_oracle(tmp_path, mg):
+    """Coulomb_supercell_type 1 (RCL = 1, 2, 2, softened cuboid): the GPU's
+    separable weights against the oracle's FFT restatement of
+    B_coulomb_supercell_fft.c."""
+    import cases
+    d = cases.commensurate(mg, tmp_path)
+    p, geo = inputs.load(d)
+    assert p["Coulomb_supercell_type"] == 1 and p["Softening"] == 1
+    pr_o = pipeline.prepare(p, geo)
+    nv, nc = 2 * p["N_VB"], 2 * p["N_CB"]
+    rng = np.random.default_rng(40 + mg)
+    v = rng.normal(size=(pr_o.n_h, nv + nc)) + 1j * rng.normal(size=(pr_o.n_h, nv + nc))
+    v /= np.linalg.norm(v, axis=0)
+    NC = (p["N_C_Gx"], p["N_C_Gy"], p["N_C_Gz"])
+    ref = coulomb.coulomb_matrix_elements(pr_o.basis, pr_o.geo, pr_o.params, v, nv, nc, NC, cme=p["CME"], ranks=2,
+                                          cell_type=1, softening=p["Softening"], sigma=p["Sigma_softening"])
+    got = q.Problem(d).coulomb(v, nv, nc, madelung_ranks=2)
+    for k in ("hh", "ee", "eh_direct", "eh_exchange"):
+        scale = np.abs(ref[k]).max()
+        assert scale > 0
+        assert np.abs(got[k] - ref[k]).max() / scale < 1e-11, k
+
+
+@pytest.mark.parametrize("example", ["prism_111", "truncated_pyramid"])
+def test_coulomb_golden_direct_terms(example):
+    d = os.path.join(os.path.dirname(GOLDEN), example)
+    gold = json.load(open(os.path.join(d, "coulomb_direct.json")))
+    prob = q.Problem(d)
     w, v = prob.solve(q.QD_PREC_FP64)
     nv, nc = gold["n_vb_states"], gold["n_cb_states"]
     out = prob.coulomb(v, nv, nc, madelung_ranks=gold["ranks"])
