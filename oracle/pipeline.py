@@ -42,7 +42,8 @@ def prepare(p, geo):
             chi_es = [None] + [chi_s[s].copy() for s in range(1, ns)]  # main:425-442
         else:
             chi_es = [None] + [shapes.chi_table(pr.basis, geo, s, 0, soft, sig) for s in range(1, ns)]
-        eps_s = strain.strain_region(pr.strain_basis, geo, pr.params, chi_s, p["Isotropic"])
+        eps_s = strain.strain_region(pr.strain_basis, geo, pr.params, chi_s, p["Isotropic"], p["Elastic_const"],
+                                     p["Elastic_const_order"])
         if pr.strain_type == 1:  # main:587-600, 634-646
             def down(t):
                 return strain.downsample_commensurate(t, pr.basis, pr.strain_basis, geo, soft, sig)

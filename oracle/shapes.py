@@ -5,10 +5,15 @@ Follows ``code/source/8_band/basis_set.c:23-90``,
 ``code/source/8_band/characteristic_function_fourier_integrals.c:28-153``
 (test infrastructure).
 
-Shapes implemented: 0 cuboid, 4 lens (hemi-ellipsoid), 5 pyramid, 6 truncated
-pyramid, 16 N-sided prism, 17 quantum well.  Every function is scalar and is
-vectorised with ``numpy.vectorize`` by ``chi_table``; the oracle is meant for
-small grids.
+All 19 shapes of the reference: 0 cuboid, 1 sphere, 2 ellipsoid, 3
+hemisphere, 4 lens (hemi-ellipsoid), 5 rectangular pyramid, 6 truncated
+rectangular pyramid, 7 N-sided pyramid, 8 truncated N-sided pyramid, 9
+cylinder, 10 cylindrical ring, 11 cone, 12 truncated cone, 13 truncated conic
+ring, 14 elliptical cone, 15 truncated elliptical cone, 16 N-sided prism, 17
+quantum well, 18 quantum wire.  The one-dimensional integrals of the curved
+shapes (I_J0, I_2 and its variants, characteristic_function_fourier_integrals.c)
+use the restated GSL QAG of ``quadrature``.  Every function is scalar and is
+looped over by ``chi_table``; the oracle is meant for small grids.
 """
 
 import cmath
@@ -31,6 +36,11 @@ def make_basis(N, L, K=(0.0, 0.0, 0.0)):
     b = {"N": tuple(int(n) for n in N), "N_T": tuple(2 * int(n) - 1 for n in N), "K": tuple(K)}
     b["G"] = tuple(basis_grid(2 * int(n) - 1, l) for n, l in zip(N, L))
     return b
+
+
+def _lround(x):
+    """C lround: nearest integer, halves away from zero."""
+    return int(math.floor(abs(x) + 0.5)) * (1 if x >= 0 else -1)
 
 
 def sinc_pi(x):
@@ -64,6 +74,56 @@ def i_j0_gauss_legendre(alpha, beta):
     so the integrand is entire and both rules converge to rounding."""
     x = _GL_X
     return float(np.sum(_GL_W * _i_j0_integrand(alpha, beta)(x)))
+
+
+def _qag(f, lo, hi):
+    from .quadrature import qag61
+    return qag61(f, lo, hi, 1.0e-4, 1.0e-4, 1000)[0]
+
+
+def i_2(alpha, beta):
+    """I_2 = int_0^1 x J0(alpha x) exp(i beta x) dx, real and imaginary parts by
+    separate QAG calls (characteristic_function_fourier_integrals.c:217-285)."""
+    re = _qag(lambda x: x * j0(alpha * x) * np.cos(beta * x), 0.0, 1.0)
+    im = _qag(lambda x: x * j0(alpha * x) * np.sin(beta * x), 0.0, 1.0)
+    return complex(re, im)
+
+
+def i_2_gz(alpha):
+    """int_0^1 x^2 J0(alpha x) dx (characteristic_function_fourier_integrals.c:342-390)."""
+    return complex(_qag(lambda x: x * x * j0(alpha * x), 0.0, 1.0), 0.0)
+
+
+def i_2_tc(alpha, R1, R2, beta):
+    """int_{R1/(R2-R1)}^{R2/(R2-R1)} x J0((R2-R1) alpha x) exp(i beta x) dx
+    (characteristic_function_fourier_integrals.c:451-521)."""
+    lo, hi = R1 / (R2 - R1), R2 / (R2 - R1)
+    a = (R2 - R1) * alpha
+    re = _qag(lambda x: x * j0(a * x) * np.cos(beta * x), lo, hi)
+    im = _qag(lambda x: x * j0(a * x) * np.sin(beta * x), lo, hi)
+    return complex(re, im)
+
+
+def i_2_tc_gz(alpha, R1, R2):
+    """int_{R1/(R2-R1)}^{R2/(R2-R1)} x^2 J0((R2-R1) alpha x) dx
+    (characteristic_function_fourier_integrals.c:577-627)."""
+    lo, hi = R1 / (R2 - R1), R2 / (R2 - R1)
+    a = (R2 - R1) * alpha
+    return complex(_qag(lambda x: x * x * j0(a * x), lo, hi), 0.0)
+
+
+def i_2_etc(alpha, beta, f):
+    """int_f^1 x J0(alpha x) exp(i beta x / (1 - f)) dx
+    (characteristic_function_fourier_integrals.c:688-757)."""
+    b = beta / (1.0 - f)
+    re = _qag(lambda x: x * j0(alpha * x) * np.cos(b * x), f, 1.0)
+    im = _qag(lambda x: x * j0(alpha * x) * np.sin(b * x), f, 1.0)
+    return complex(re, im)
+
+
+def i_2_etc_gz(alpha, f):
+    """int_f^1 x^2 J0(alpha x) dx (characteristic_function_fourier_integrals.c:813-861)."""
+    return complex(_qag(lambda x: x * x * j0(alpha * x), f, 1.0), 0.0)
 
 
 def i_e0(a, G):
@@ -199,6 +259,29 @@ def chi(Gx0, Gy0, Gz0, geo, idx, cell, softening=0, sigma=0.0):
         r *= math.exp(-0.5 * sigma ** 2 * (Gx ** 2 + Gy ** 2 + Gz ** 2))
     shape = g["shape"]
     L1, L2, L3, L4 = g["L1"], g["L2"], g["L3"], g["L4"]
+    G_mag = math.sqrt(Gx * Gx + Gy * Gy + Gz * Gz)
+    G_par = math.sqrt(Gx * Gx + Gy * Gy)
+    I = 1j
+    J1 = lambda x: float(j1(x))  # noqa: E731
+    if shape in (10, 13):
+        # characteristic_function_fourier.c:580-620, 725-767: differences of two
+        # shapes evaluated from the unrotated G (each with its own prefactor)
+        g2 = dict(g)
+        geo2 = list(geo)
+        geo2[idx] = g2
+        if shape == 10:
+            g2["shape"] = 9
+            g2["L2"] = L3
+            r = chi(Gx0, Gy0, Gz0, geo2, idx, cell, softening, sigma)
+            g2["L1"] = L2
+            return r - chi(Gx0, Gy0, Gz0, geo2, idx, cell, softening, sigma)
+        g2["shape"] = 12
+        g2["L3"] = L4
+        r = chi(Gx0, Gy0, Gz0, geo2, idx, cell, softening, sigma)
+        g2["shape"] = 9
+        g2["L1"] = L3
+        g2["L2"] = L4
+        return r - cmath.exp(-0.5 * I * Gz * L4) * chi(Gx0, Gy0, Gz0, geo2, idx, cell, softening, sigma)
     if shape == 0:
         r *= (L1 * sinc_pi((0.5 * Gx * L1) / math.pi) * L2 * sinc_pi((0.5 * Gy * L2) / math.pi)
               * L3 * sinc_pi((0.5 * Gz * L3) / math.pi))
@@ -228,21 +311,136 @@ def chi(Gx0, Gy0, Gz0, geo, idx, cell, softening=0, sigma=0.0):
         for s in range(4):
             seg -= cmath.exp(-1.0j * Gz * L4) * pyramid_segment(Gx, Gy, Gz, s, 0, g2)
         r *= seg
+    elif shape == 1:  # sphere, radius L1
+        if abs(G_mag) < EPS:
+            r *= (4.0 * math.pi * L1 ** 3) / 3.0
+        else:
+            r *= (4.0 * math.pi * (math.sin(G_mag * L1) - G_mag * L1 * math.cos(G_mag * L1))) / G_mag ** 3
+    elif shape == 2:  # ellipsoid, semi-axes L1, L2, L3
+        Gs = math.sqrt((Gx * L1) ** 2 + (Gy * L2) ** 2 + (Gz * L3) ** 2)
+        if abs(Gs) < EPS:
+            r *= (4.0 * math.pi * L1 * L2 * L3) / 3.0
+        else:
+            r *= (4.0 * math.pi * L1 * L2 * L3 * (math.sin(Gs) - Gs * math.cos(Gs))) / Gs ** 3
+    elif shape == 3:  # hemisphere, radius L1, base at the centre
+        sph = 2.0 * math.pi * (math.sin(G_mag * L1) - G_mag * L1 * math.cos(G_mag * L1)) / (G_mag ** 3) \
+            if abs(G_mag) >= EPS else 0.0
+        if abs(G_mag) < EPS:
+            r *= (2.0 * math.pi * L1 ** 3) / 3.0
+        elif abs(G_par) < EPS and abs(Gz) > EPS:
+            r *= sph - ((2.0 * math.pi * I * L1 ** 2) / Gz) * (
+                0.5 - (L1 * Gz * math.sin(L1 * Gz) + math.cos(L1 * Gz) - 1.0) / (Gz * L1) ** 2)
+        elif abs(Gz) < EPS and abs(G_par) > EPS:
+            r *= sph
+        else:
+            r *= (sph - (2.0 * math.pi * I * L1 * J1(G_par * L1)) / (G_par * Gz)
+                  + (2.0 * math.pi * I * L1 ** 2 * i_j0(Gz * L1, G_par * L1)) / Gz)
+    elif shape == 7:  # N-sided pyramid: N = lround(L3 / 10), circumradius-type length L1, height L2
+        n = _lround(0.1 * L3)
+        r *= sum(pyramid_segment(Gx, Gy, Gz, k, n, g) for k in range(n))
+    elif shape == 8:  # truncated N-sided pyramid: N = lround(L4 / 10)
+        n = _lround(0.1 * L4)
+        g2 = dict(g)
+        g2["L2"] = (L1 * L3) / (L1 - L2)
+        seg = sum(pyramid_segment(Gx, Gy, Gz, k, n, g2) for k in range(n))
+        g2["L1"] = L2
+        g2["L2"] = (L3 * L2) / (L1 - L2)
+        for k in range(n):
+            seg -= cmath.exp(-1.0 * I * Gz * L3) * pyramid_segment(Gx, Gy, Gz, k, n, g2)
+        r *= seg
+    elif shape == 9:  # cylinder, radius L1, height L2 (centred)
+        if abs(G_mag) < EPS:
+            r *= math.pi * L1 ** 2 * L2
+        elif abs(G_par) < EPS and abs(Gz) > EPS:
+            r *= 2.0 * math.pi * L1 ** 2 * math.sin(0.5 * Gz * L2) / Gz
+        elif abs(Gz) < EPS and abs(G_par) > EPS:
+            r *= (2.0 * math.pi * L1 * L2 * J1(G_par * L1)) / G_par
+        else:
+            r *= (4.0 * math.pi * L1 * math.sin(0.5 * Gz * L2) * J1(G_par * L1)) / (G_par * Gz)
+    elif shape == 11:  # cone, base radius L1, height L2
+        if abs(G_mag) < EPS:
+            r *= (math.pi * L1 ** 2 * L2) / 3.0
+        elif abs(G_par) < EPS:
+            r *= (2.0 * I * math.pi * L1 ** 2 * ((1.0 - I * Gz * L2 - cmath.exp(-1.0 * I * Gz * L2)) / (Gz * L2) ** 2
+                                                 - 0.5)) / Gz
+        elif abs(Gz) < EPS:
+            r *= (2.0 * math.pi * L1 ** 2 * L2) * (J1(G_par * L1) / (G_par * L1) - i_2_gz(G_par * L1))
+        else:
+            r *= ((2.0 * math.pi * L1 * L1 * I * cmath.exp(-1.0 * I * Gz * L2) * i_2(G_par * L1, Gz * L2)) / Gz
+                  - (2.0 * math.pi * I * L1 * J1(G_par * L1)) / (G_par * Gz))
+    elif shape == 12:  # truncated cone, base radius L1, top radius L2, height L3
+        if abs(G_mag) < EPS:
+            r *= (math.pi * L3 * (L1 * L1 + L1 * L2 + L2 * L2)) / 3.0
+        elif abs(G_par) < EPS:
+            e = cmath.exp(-1.0 * I * Gz * L3)
+            r *= ((2.0 * I * math.pi) / Gz) * (
+                (0.5 * L2 ** 2 * (e - 1.0))
+                + ((L1 - L2) ** 2 / (Gz * L3) ** 2 * (e * ((I * Gz * L2 * L3) / (L1 - L2) - 1.0)
+                                                       + (1.0 - (I * L1 * Gz * L3) / (L1 - L2))))
+                - (0.5 * (L1 ** 2 - L2 ** 2)))
+        elif abs(Gz) < EPS:
+            r *= (2.0 * math.pi * L3) * ((L2 * J1(G_par * L2) / G_par)
+                                         - ((L1 - L2) ** 2 * i_2_tc_gz(G_par, L2, L1))
+                                         + ((L1 / (L1 - L2)) * (L1 * J1(G_par * L1) - L2 * J1(G_par * L2)) / G_par))
+        else:
+            r *= (2.0 * I * math.pi / Gz) * (
+                (L2 * (cmath.exp(-1.0 * I * Gz * L3) - 1.0) * J1(G_par * L2) / G_par)
+                + ((L1 - L2) ** 2 * cmath.exp((-1.0 * I * Gz * L3 * L1) / (L1 - L2)) * i_2_tc(G_par, L2, L1, Gz * L3))
+                - ((L1 * J1(G_par * L1) - L2 * J1(G_par * L2)) / G_par))
+    elif shape == 14:  # elliptical cone, semi-axes L1, L2, height L3
+        Gp = math.sqrt((Gx * L1) ** 2 + (Gy * L2) ** 2)
+        if abs(G_mag) < EPS:
+            r *= (math.pi * L1 * L2 * L3) / 3.0
+        elif abs(Gp) < EPS:
+            r *= (1.0 / Gz) * (2.0 * I * math.pi * L1 * L2 * ((1.0 - I * Gz * L3 - cmath.exp(-1.0 * I * Gz * L3))
+                                                              / (Gz * L3) ** 2 - 0.5))
+        elif abs(Gz) < EPS:
+            r *= (2.0 * math.pi * L1 * L2 * L3) * (J1(Gp) / Gp - i_2_gz(Gp))
+        else:
+            r *= ((2.0 * math.pi * L1 * L2 * I * cmath.exp(-1.0 * I * Gz * L3) * i_2(Gp, Gz * L3)) / Gz
+                  - (2.0 * math.pi * I * L1 * L2 * J1(Gp)) / (Gp * Gz))
+    elif shape == 15:  # truncated elliptical cone, semi-axes L1, L2, top ratio f = L3 / L1, height L4
+        Gp = math.sqrt((Gx * L1) ** 2 + (Gy * L2) ** 2)
+        f = L3 / L1
+        if abs(G_mag) < EPS:
+            r *= (math.pi * L1 * L2 * L4 * (1.0 + f + f ** 2)) / 3.0
+        elif abs(Gp) < EPS:
+            e = cmath.exp(-1.0 * I * Gz * L4)
+            r *= (2.0 * math.pi * I * L1 * L2 * (
+                (0.5 * f ** 2 * (e - 1.0))
+                + ((f - 1.0) / (Gz * Gz * L4 * L4) * (e * (-1.0 * I * Gz * L4 * f - f + 1.0) + (I * Gz * L4 + f - 1.0)))
+                - (0.5 * (1.0 - f ** 2))) / Gz)
+        elif abs(Gz) < EPS:
+            r *= (2.0 * math.pi * L1 * L2 * L4) * ((f * J1(f * Gp) / Gp) - (1.0 * i_2_etc_gz(Gp, f)) / (1.0 - f)
+                                                   + ((J1(Gp) - f * J1(f * Gp)) / ((1.0 - f) * Gp)))
+        else:
+            r *= ((2.0 * I * math.pi * L1 * L2) / Gz) * (
+                (f * (cmath.exp(-1.0 * I * Gz * L4) - 1.0) * J1(f * Gp) / Gp)
+                + (cmath.exp(-1.0 * I * Gz * L4 / (1.0 - f)) * i_2_etc(Gp, Gz * L4, f))
+                - ((J1(Gp) - f * J1(f * Gp)) / Gp))
+    elif shape == 18:  # quantum wire along axis lround(L1 / 10), cross-section L2 x L3
+        d = _lround(0.1 * L1)
+        cellL = (g0["L1"], g0["L2"], g0["L3"]) if cell == 0 else (g0["SL1"], g0["SL2"], g0["SL3"])
+        lens = {0: (cellL[0], L2, L3), 1: (L2, cellL[1], L3), 2: (L2, L3, cellL[2])}.get(d)
+        if lens is not None:  # another axis index leaves the prefactor alone, as in the reference
+            r *= (lens[0] * sinc_pi((0.5 * Gx * lens[0]) / math.pi) * lens[1] * sinc_pi((0.5 * Gy * lens[1]) / math.pi)
+                  * lens[2] * sinc_pi((0.5 * Gz * lens[2]) / math.pi))
     elif shape == 16:
-        n = int(round(0.1 * L3))
+        n = _lround(0.1 * L3)
         r *= sum(prism_segment(Gx, Gy, Gz, s, n, g) for s in range(n))
     elif shape == 17:
-        d = int(round(0.1 * L1))
+        d = _lround(0.1 * L1)
         if cell == 0:
             dims = (g0["L1"], g0["L2"], g0["L3"])
         else:
             dims = (g0["SL1"], g0["SL2"], g0["SL3"])
-        lens = list(dims)
-        lens[d] = L2
-        r *= (lens[0] * sinc_pi((0.5 * Gx * lens[0]) / math.pi) * lens[1] * sinc_pi((0.5 * Gy * lens[1]) / math.pi)
-              * lens[2] * sinc_pi((0.5 * Gz * lens[2]) / math.pi))
+        if d in (0, 1, 2):  # another axis index leaves the prefactor alone, as in the reference
+            lens = list(dims)
+            lens[d] = L2
+            r *= (lens[0] * sinc_pi((0.5 * Gx * lens[0]) / math.pi) * lens[1]
+                  * sinc_pi((0.5 * Gy * lens[1]) / math.pi) * lens[2] * sinc_pi((0.5 * Gz * lens[2]) / math.pi))
     else:
-        raise NotImplementedError("shape %d is not in the oracle" % shape)
+        raise ValueError("unknown shape %d" % shape)
     return r
 
 

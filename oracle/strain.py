@@ -1,8 +1,9 @@
 """Oracle restatement of the strain, piezoelectric and convolution tables.
 
 Follows (test infrastructure):
-  * ``strain_region_reciprocal_space.c:24-418`` + ``strain_fourier_coefficient.c:23-390``
-    (position-independent elastic constants only),
+  * ``strain_region_reciprocal_space.c:24-418`` + ``strain_fourier_coefficient.c:23-470``
+    (position-independent elastic constants, and the perturbative position-dependent
+    ones with ``convolutions_strain_correction.c:23-358``),
   * ``piezo_region_reciprocal_space.c:23-787`` + ``piezo_fourier_coefficient.c:24-132``,
   * ``strain_reciprocal_space.c:23-230`` / ``piezo_reciprocal_space.c:23-186``
     (free-length downsampling; the identity copy when the cells coincide),
@@ -58,18 +59,123 @@ def strain_factor(comp, Gx, Gy, Gz, p0, isotropic):
     return np.where(zero, f0, f)
 
 
-def strain_region(basis, geo, params, chi_strain, isotropic):
-    """epsilon_ij(G) on the strain grid (strain_region_reciprocal_space.c:24-140)."""
+def green_tensor(comp, Gx, Gy, Gz, G, ssum, p0):
+    """greens_function_tensor (strain_fourier_coefficient.c:394-470): the
+    matrix material's elastic Green tensor component ij at G (G != 0)."""
+    i, j = _IJ[comp]
+    G3 = (Gx, Gy, Gz)
+    Gi, Gj = G3[i], G3[j]
+    C11, C12, C44 = p0["C11"], p0["C12"], p0["C44"]
+    D = C11 - C12 - 2.0 * C44
+    dij = 1.0 if i == j else 0.0
+    return (dij / (C44 * G * G + D * Gi * Gi)) - ((C12 + C44) * Gi * Gj / (
+        (1.0 + (C12 + C44) * ssum) * (C44 * G * G + D * Gi * Gi) * (C44 * G * G + D * Gj * Gj)))
+
+
+def _order0_factor(comp, Gx, Gy, Gz, p0, ps, isotropic):
+    """Zeroth-order factor of the position-dependent elastic constants
+    (strain_fourier_coefficient.c:177-224): the shape's own C11, C12, C44 in the
+    numerators, the matrix's in the Green tensor."""
+    i, j = _IJ[comp]
+    G3 = (Gx, Gy, Gz)
+    Gi, Gj = G3[i], G3[j]
+    G = np.sqrt(Gx ** 2 + Gy ** 2 + Gz ** 2)
+    dij = 1.0 if i == j else 0.0
+    C11, C12, C44 = p0["C11"], p0["C12"], p0["C44"]
+    zero = np.abs(G) < EPS
+    Gs = np.where(zero, 1.0, G)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if isotropic == 1:
+            f0 = dij * (-1 * (3.0 * ps["C12"] + 2.0 * ps["C44"]) / (3.0 * C12 + 6.0 * C44))
+            f = -((3.0 * ps["C12"] + 2.0 * ps["C44"]) * Gi * Gj) / ((C12 + 2.0 * C44) * Gs * Gs)
+        else:
+            D = C11 - C12 - 2.0 * C44
+            s0 = 1.0 / (C44 + D / 3.0)
+            f0 = dij * ((-0.5 * (ps["C11"] + 2.0 * ps["C12"]) / 3.0) * (2.0 / (C44 + D / 3.0))
+                        / (1.0 + (C12 + C44) * s0))
+            ssum = ((Gx * Gx) / (C44 * Gs * Gs + D * Gx * Gx) + (Gy * Gy) / (C44 * Gs * Gs + D * Gy * Gy)
+                    + (Gz * Gz) / (C44 * Gs * Gs + D * Gz * Gz))
+            f = -(0.5 * (ps["C11"] + 2.0 * ps["C12"]) * (2.0 * C44 * Gs * Gs + D * (Gi * Gi + Gj * Gj)) * Gi * Gj) / (
+                (1.0 + (C12 + C44) * ssum) * (C44 * Gs * Gs + D * Gi * Gi) * (C44 * Gs * Gs + D * Gj * Gj))
+    return np.where(zero, f0, f)
+
+
+def _correction_factor(comp, Gx, Gy, Gz, p0, ps, isotropic):
+    """Factor multiplying chi_s (*) (previous correction) for correction orders
+    >= 1 (strain_fourier_coefficient.c:226-386)."""
+    G = np.sqrt(Gx ** 2 + Gy ** 2 + Gz ** 2)
+    zero = np.abs(G) < EPS
+    Gs = np.where(zero, 1.0, G)
+    C11, C12, C44 = p0["C11"], p0["C12"], p0["C44"]
+    D = C11 - C12 - 2.0 * C44
+    dC11, dC12, dC44 = ps["C11"] - C11, ps["C12"] - C12, ps["C44"] - C44
+    i, j = _IJ[comp]
+    if isotropic == 1:
+        f0 = -(1.0 / (3.0 * C44)) * (ps["C11"] - C11 + 2.0 * ps["C12"] - 2.0 * C12) if i == j else 0.0
+    else:
+        s0 = 1.0 / (C44 + D / 3.0)
+        f0 = -(s0 / 3.0) * (ps["C11"] - C11 + 2.0 * ps["C12"] - 2.0 * C12) if i == j else 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ssum = ((Gx * Gx) / (C44 * Gs * Gs + D * Gx * Gx) + (Gy * Gy) / (C44 * Gs * Gs + D * Gy * Gy)
+                + (Gz * Gz) / (C44 * Gs * Gs + D * Gz * Gz))
+
+        def g(c):
+            return green_tensor(c, Gx, Gy, Gz, Gs, ssum, p0)
+        G3 = (Gx, Gy, Gz)
+        Gi, Gj = G3[i], G3[j]
+        if comp == "xx":
+            f = -1.0 * (Gi * ((dC11 * Gx * g("xx")) + (dC12 * Gy * g("xy")) + (dC12 * Gz * g("xz"))))
+        elif comp == "yy":
+            f = -1.0 * (Gi * ((dC12 * Gx * g("xy")) + (dC11 * Gy * g("yy")) + (dC12 * Gz * g("yz"))))
+        elif comp == "zz":
+            f = -1.0 * (Gi * ((dC12 * Gx * g("xz")) + (dC12 * Gy * g("yz")) + (dC11 * Gz * g("zz"))))
+        elif comp == "yz":
+            f = -0.5 * dC44 * (Gi * ((Gz * g("yz")) + (Gy * g("zz"))) + Gj * ((Gz * g("yy")) + (Gy * g("yz"))))
+        elif comp == "xz":
+            f = -0.5 * dC44 * (Gi * ((Gz * g("xz")) + (Gx * g("zz"))) + Gj * ((Gz * g("xx")) + (Gx * g("xz"))))
+        else:
+            f = -0.5 * dC44 * (Gi * ((Gy * g("xy")) + (Gx * g("yy"))) + Gj * ((Gy * g("xx")) + (Gx * g("xy"))))
+    return np.where(zero, f0, f)
+
+
+def strain_region(basis, geo, params, chi_strain, isotropic, elastic_const=0, order=0):
+    """epsilon_ij(G) on the strain grid (strain_region_reciprocal_space.c:24-418).
+
+    elastic_const 0: position-independent elastic constants (the matrix's).
+    elastic_const 1: the perturbative treatment of each shape's own constants,
+    per shape: the initial term eps0 chi delta_ij, the zeroth-order term with
+    the shape's constants, then ``order`` corrections, each the convolution of
+    chi_s with the previous correction (zero-padded FFT, central block) times
+    the Green-tensor factor of the constant differences."""
     if isotropic != 0:
         for p in params:
             p["C44"] = 0.5 * (p["C11"] - p["C12"])
     Gx, Gy, Gz = _grids(basis)
     eps = {c: np.zeros(Gx.shape, dtype=np.complex128) for c in COMPONENTS}
-    fac = {c: strain_factor(c, Gx, Gy, Gz, params[0], isotropic) for c in COMPONENTS}
+    if elastic_const == 0:
+        fac = {c: strain_factor(c, Gx, Gy, Gz, params[0], isotropic) for c in COMPONENTS}
+        for s in range(1, len(geo)):
+            eps0 = (params[geo[s]["embedded"]]["a"] - params[s]["a"]) / params[0]["a"]
+            for c in COMPONENTS:
+                eps[c] += eps0 * chi_strain[s] * fac[c]
+        return eps
+    n = Gx.shape
     for s in range(1, len(geo)):
-        eps0 = (params[geo[s]["embedded"]]["a"] - params[s]["a"]) / params[0]["a"]
+        ps = params[s]
+        eps0 = (params[geo[s]["embedded"]]["a"] - ps["a"]) / params[0]["a"]
         for c in COMPONENTS:
-            eps[c] += eps0 * chi_strain[s] * fac[c]
+            if _IJ[c][0] == _IJ[c][1]:
+                eps[c] += eps0 * chi_strain[s]
+        corr = {c: eps0 * chi_strain[s] * _order0_factor(c, Gx, Gy, Gz, params[0], ps, isotropic)
+                for c in COMPONENTS}
+        for c in COMPONENTS:
+            eps[c] += corr[c]
+        X = np.fft.fftn(pad(chi_strain[s]))
+        for _ in range(order):
+            conv = {c: conv_hat(X, np.fft.fftn(pad(corr[c])), n) for c in COMPONENTS}
+            corr = {c: conv[c] * _correction_factor(c, Gx, Gy, Gz, params[0], ps, isotropic) for c in COMPONENTS}
+            for c in COMPONENTS:
+                eps[c] += corr[c]
     return eps
 
 

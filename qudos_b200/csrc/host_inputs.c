@@ -73,6 +73,7 @@ static int apply_key(qd_params *p, const char *key, const char *value, int *err)
         case 18: p->strain = (int)iv; break;
         case 19: p->isotropic = (int)iv; break;
         case 20: p->elastic_const = (int)iv; break;
+        case 21: p->elastic_order = (int)iv; break;
         case 22: p->piezo = (int)iv; break;
         case 26: p->cme = (int)iv; break;
         case 27: p->coulomb_type = (int)iv; break;

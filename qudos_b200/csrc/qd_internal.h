@@ -22,7 +22,7 @@ typedef struct {
     int strain_type, coulomb_type;
     int n_vb, n_cb;
     double T, F[3], K[3];
-    int strain, isotropic, elastic_const, piezo, cme, softening;
+    int strain, isotropic, elastic_const, elastic_order, piezo, cme, softening;
     double sigma;
     int eigensolver;
 } qd_params;

@@ -74,6 +74,32 @@ __device__ double i_j0(double alpha, double beta) {
     return s;
 }
 
+// int_lo^hi x^p J0(a x) exp(i b x) dx, p = 1 or 2: the one-dimensional integrals
+// of the cones (I_2, I_2_Gz, I_2_TC, I_2_TC_Gz, I_2_ETC, I_2_ETC_Gz,
+// characteristic_function_fourier_integrals.c:217-861), which the reference
+// evaluates with GSL's adaptive 61-point Gauss-Kronrod rule to 1e-4.  The
+// integrands are entire; a composite 96-point Gauss-Legendre rule with one
+// panel per 40 radians of |a| + |b| over the interval reproduces the exact
+// integral to rounding, and so the adaptive rule's value wherever it meets its
+// tolerance (the oracle restates the adaptive rule).
+__device__ zc bessel_moment(double lo, double hi, double a, double b, int p) {
+    const double span = hi - lo;
+    const int panels = 1 + (int)((fabs(a) + fabs(b)) * fabs(span) / 40.0);
+    const double h = span / panels;
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < panels; k++) {
+        for (int i = 0; i < QD_GL_N; i++) {
+            const double x = lo + h * (k + c_gl_x[i]);
+            double f = c_gl_w[i] * j0(a * x) * (p == 2 ? x * x : x);
+            double sn, cs;
+            sincos(b * x, &sn, &cs);
+            re += f * cs;
+            im += f * sn;
+        }
+    }
+    return zc(h * re, h * im);
+}
+
 __device__ inline double sinc_pi(double x) {  // gsl_sf_sinc: sin(pi x)/(pi x)
     if (fabs(x) < 1e-8) return 1.0 - (M_PI * M_PI) * x * x / 6.0;
     return sinpi(x) / (M_PI * x);
@@ -179,6 +205,41 @@ __device__ zc prism_segment(double Gx0, double Gy0, double Gz0, int idx_side, in
     return pre * ((1.0 / p) * tp - (1.0 / m) * tm);
 }
 
+// Cylinder of radius R and height H centred in z (characteristic_function_fourier.c:532-578).
+__device__ zc cylinder_factor(double Gx, double Gy, double Gz, double R, double H) {
+    const double G_mag = sqrt(Gx * Gx + Gy * Gy + Gz * Gz), G_par = sqrt(Gx * Gx + Gy * Gy);
+    if (fabs(G_mag) < QD_EPS) return zc(M_PI * R * R * H);
+    if (fabs(G_par) < QD_EPS && fabs(Gz) > QD_EPS) return zc(2.0 * M_PI * R * R * sin(0.5 * Gz * H) / Gz);
+    if (fabs(Gz) < QD_EPS && fabs(G_par) > QD_EPS) return zc((2.0 * M_PI * R * H * j1(G_par * R)) / G_par);
+    return zc((4.0 * M_PI * R * sin(0.5 * Gz * H) * j1(G_par * R)) / (G_par * Gz));
+}
+
+// Truncated cone, base radius R1 on z = 0, top radius R2 at z = H
+// (characteristic_function_fourier.c:671-723).
+__device__ zc truncated_cone_factor(double Gx, double Gy, double Gz, double R1, double R2, double H) {
+    const double G_mag = sqrt(Gx * Gx + Gy * Gy + Gz * Gz), G_par = sqrt(Gx * Gx + Gy * Gy);
+    const zc I(0.0, 1.0);
+    if (fabs(G_mag) < QD_EPS) return zc((M_PI * H * (R1 * R1 + R1 * R2 + R2 * R2)) / 3.0);
+    const double d = R1 - R2;
+    if (fabs(G_par) < QD_EPS) {
+        const zc e = cexpi(-Gz * H);
+        const zc t = 0.5 * R2 * R2 * (e - zc(1.0)) +
+                     (d * d / ((Gz * H) * (Gz * H))) *
+                         (e * (I * ((Gz * R2 * H) / d) - zc(1.0)) + (zc(1.0) - I * ((R1 * Gz * H) / d))) -
+                     zc(0.5 * (R1 * R1 - R2 * R2));
+        return zc(0.0, 2.0 * M_PI / Gz) * t;
+    }
+    if (fabs(Gz) < QD_EPS) {
+        const zc i2 = bessel_moment(R2 / d, R1 / d, d * G_par, 0.0, 2);
+        return (2.0 * M_PI * H) * (zc(R2 * j1(G_par * R2) / G_par) - (d * d) * i2 +
+                                   zc((R1 / d) * (R1 * j1(G_par * R1) - R2 * j1(G_par * R2)) / G_par));
+    }
+    const zc i2 = bessel_moment(R2 / d, R1 / d, d * G_par, Gz * H, 1);
+    const zc t = (R2 * j1(G_par * R2) / G_par) * (cexpi(-Gz * H) - zc(1.0)) +
+                 (d * d) * cexpi((-Gz * H * R1) / d) * i2 - zc((R1 * j1(G_par * R1) - R2 * j1(G_par * R2)) / G_par);
+    return zc(0.0, 2.0 * M_PI / Gz) * t;
+}
+
 // characteristic_function_fourier.c:58-1110 for one wave vector.  cell: 0
 // electronic cell, 1/2 strain cell, 3 Coulomb cell (volume normalisation).
 __device__ zc chi_point(double Gx0, double Gy0, double Gz0, const geo_t *geo, int s, int cell, int softening,
@@ -239,6 +300,138 @@ __device__ zc chi_point(double Gx0, double Gy0, double Gz0, const geo_t *geo, in
             r *= seg;
             break;
         }
+        case 1: {  // sphere, radius L1
+            const double G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz);
+            if (fabs(G) < QD_EPS) r *= (4.0 * M_PI * g.L1 * g.L1 * g.L1) / 3.0;
+            else r *= (4.0 * M_PI * (sin(G * g.L1) - G * g.L1 * cos(G * g.L1))) / (G * G * G);
+            break;
+        }
+        case 2: {  // ellipsoid, semi-axes L1, L2, L3
+            const double a = Gx * g.L1, b = Gy * g.L2, c = Gz * g.L3, G = sqrt(a * a + b * b + c * c);
+            if (fabs(G) < QD_EPS) r *= (4.0 * M_PI * g.L1 * g.L2 * g.L3) / 3.0;
+            else r *= (4.0 * M_PI * g.L1 * g.L2 * g.L3 * (sin(G) - G * cos(G))) / (G * G * G);
+            break;
+        }
+        case 3: {  // hemisphere, radius L1, base at the centre
+            const double R = g.L1, G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz), Gp = sqrt(Gx * Gx + Gy * Gy);
+            if (fabs(G) < QD_EPS) {
+                r *= (2.0 * M_PI * R * R * R) / 3.0;
+            } else {
+                const double sph = (2.0 * M_PI * (sin(G * R) - G * R * cos(G * R))) / (G * G * G);
+                if (fabs(Gp) < QD_EPS && fabs(Gz) > QD_EPS) {
+                    const double t = 0.5 - (R * Gz * sin(R * Gz) + cos(R * Gz) - 1.0) / ((Gz * R) * (Gz * R));
+                    r *= zc(sph, -(2.0 * M_PI * R * R / Gz) * t);
+                } else if (fabs(Gz) < QD_EPS && fabs(Gp) > QD_EPS) {
+                    r *= sph;
+                } else {
+                    const double t = -(2.0 * M_PI * R * j1(Gp * R)) / (Gp * Gz) +
+                                     (2.0 * M_PI * R * R * i_j0(Gz * R, Gp * R)) / Gz;
+                    r *= zc(sph, t);
+                }
+            }
+            break;
+        }
+        case 7: {  // N-sided pyramid, N = lround(L3 / 10), inradius L1, height L2
+            const int n = (int)lround(0.1 * g.L3);
+            zc seg;
+            for (int k = 0; k < n; k++) seg += pyramid_segment(Gx, Gy, Gz, k, n, g.L1, g.L2, g.L3);
+            r *= seg;
+            break;
+        }
+        case 8: {  // truncated N-sided pyramid, N = lround(L4 / 10): inradii L1 (base), L2 (top), height L3
+            const int n = (int)lround(0.1 * g.L4);
+            zc seg;
+            const double h1 = (g.L1 * g.L3) / (g.L1 - g.L2), h2 = (g.L3 * g.L2) / (g.L1 - g.L2);
+            for (int k = 0; k < n; k++) seg += pyramid_segment(Gx, Gy, Gz, k, n, g.L1, h1, g.L3);
+            const zc ez = cexpi(-Gz * g.L3);
+            for (int k = 0; k < n; k++) seg -= ez * pyramid_segment(Gx, Gy, Gz, k, n, g.L2, h2, g.L3);
+            r *= seg;
+            break;
+        }
+        case 9:  // cylinder, radius L1, height L2
+            r *= cylinder_factor(Gx, Gy, Gz, g.L1, g.L2);
+            break;
+        case 10:  // cylindrical ring, radii L1 > L2, height L3
+            r *= cylinder_factor(Gx, Gy, Gz, g.L1, g.L3) - cylinder_factor(Gx, Gy, Gz, g.L2, g.L3);
+            break;
+        case 11: {  // cone, base radius L1, height L2
+            const double R = g.L1, H = g.L2, G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz), Gp = sqrt(Gx * Gx + Gy * Gy);
+            const zc I(0.0, 1.0);
+            if (fabs(G) < QD_EPS) {
+                r *= (M_PI * R * R * H) / 3.0;
+            } else if (fabs(Gp) < QD_EPS) {
+                const zc t = (zc(1.0) - I * (Gz * H) - cexpi(-Gz * H)) / ((Gz * H) * (Gz * H)) - zc(0.5);
+                r *= zc(0.0, 2.0 * M_PI * R * R / Gz) * t;
+            } else if (fabs(Gz) < QD_EPS) {
+                r *= (2.0 * M_PI * R * R * H) * (zc(j1(Gp * R) / (Gp * R)) - bessel_moment(0.0, 1.0, Gp * R, 0.0, 2));
+            } else {
+                r *= zc(0.0, 2.0 * M_PI * R * R / Gz) * cexpi(-Gz * H) * bessel_moment(0.0, 1.0, Gp * R, Gz * H, 1) -
+                     zc(0.0, (2.0 * M_PI * R * j1(Gp * R)) / (Gp * Gz));
+            }
+            break;
+        }
+        case 12:  // truncated cone, base radius L1, top radius L2, height L3
+            r *= truncated_cone_factor(Gx, Gy, Gz, g.L1, g.L2, g.L3);
+            break;
+        case 13:  // truncated conic ring: truncated cone (L1, L2, height L4) less a cylinder of radius L3
+            r *= truncated_cone_factor(Gx, Gy, Gz, g.L1, g.L2, g.L4) -
+                 cexpi(-0.5 * Gz * g.L4) * cylinder_factor(Gx, Gy, Gz, g.L3, g.L4);
+            break;
+        case 14: {  // elliptical cone, semi-axes L1, L2, height L3
+            const double A = g.L1 * g.L2, H = g.L3, G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz);
+            const double Gp = sqrt((Gx * g.L1) * (Gx * g.L1) + (Gy * g.L2) * (Gy * g.L2));
+            const zc I(0.0, 1.0);
+            if (fabs(G) < QD_EPS) {
+                r *= (M_PI * A * H) / 3.0;
+            } else if (fabs(Gp) < QD_EPS) {
+                const zc t = (zc(1.0) - I * (Gz * H) - cexpi(-Gz * H)) / ((Gz * H) * (Gz * H)) - zc(0.5);
+                r *= zc(0.0, 2.0 * M_PI * A / Gz) * t;
+            } else if (fabs(Gz) < QD_EPS) {
+                r *= (2.0 * M_PI * A * H) * (zc(j1(Gp) / Gp) - bessel_moment(0.0, 1.0, Gp, 0.0, 2));
+            } else {
+                r *= zc(0.0, 2.0 * M_PI * A / Gz) * cexpi(-Gz * H) * bessel_moment(0.0, 1.0, Gp, Gz * H, 1) -
+                     zc(0.0, (2.0 * M_PI * A * j1(Gp)) / (Gp * Gz));
+            }
+            break;
+        }
+        case 15: {  // truncated elliptical cone: semi-axes L1, L2, top ratio f = L3 / L1, height L4
+            const double A = g.L1 * g.L2, H = g.L4, f = g.L3 / g.L1, G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz);
+            const double Gp = sqrt((Gx * g.L1) * (Gx * g.L1) + (Gy * g.L2) * (Gy * g.L2));
+            const zc I(0.0, 1.0);
+            if (fabs(G) < QD_EPS) {
+                r *= (M_PI * A * H * (1.0 + f + f * f)) / 3.0;
+            } else if (fabs(Gp) < QD_EPS) {
+                const zc e = cexpi(-Gz * H);
+                const zc t = 0.5 * f * f * (e - zc(1.0)) +
+                             ((f - 1.0) / (Gz * Gz * H * H)) *
+                                 (e * zc(-f + 1.0, -Gz * H * f) + zc(f - 1.0, Gz * H)) -
+                             zc(0.5 * (1.0 - f * f));
+                r *= zc(0.0, 2.0 * M_PI * A / Gz) * t;
+            } else if (fabs(Gz) < QD_EPS) {
+                r *= (2.0 * M_PI * A * H) * (zc(f * j1(f * Gp) / Gp) - bessel_moment(f, 1.0, Gp, 0.0, 2) / (1.0 - f) +
+                                             zc((j1(Gp) - f * j1(f * Gp)) / ((1.0 - f) * Gp)));
+            } else {
+                const zc t = (f * j1(f * Gp) / Gp) * (cexpi(-Gz * H) - zc(1.0)) +
+                             cexpi(-Gz * H / (1.0 - f)) * bessel_moment(f, 1.0, Gp, Gz * H / (1.0 - f), 1) -
+                             zc((j1(Gp) - f * j1(f * Gp)) / Gp);
+                r *= zc(0.0, 2.0 * M_PI * A / Gz) * t;
+            }
+            break;
+        }
+        case 18: {  // quantum wire along axis lround(L1 / 10), cross-section L2 x L3
+            const int d = (int)lround(0.1 * g.L1);
+            double c[3];
+            if (cell == 0) { c[0] = g0.L1; c[1] = g0.L2; c[2] = g0.L3; }
+            else { c[0] = g0.SL1; c[1] = g0.SL2; c[2] = g0.SL3; }
+            double l[3];
+            if (d == 0) { l[0] = c[0]; l[1] = g.L2; l[2] = g.L3; }
+            else if (d == 1) { l[0] = g.L2; l[1] = c[1]; l[2] = g.L3; }
+            else if (d == 2) { l[0] = g.L2; l[1] = g.L3; l[2] = c[2]; }
+            else break;  // another axis index leaves the prefactor alone, as in the reference
+            r *= l[0] * sinc_pi((0.5 * Gx * l[0]) / M_PI) * l[1] * sinc_pi((0.5 * Gy * l[1]) / M_PI) * l[2] *
+                 sinc_pi((0.5 * Gz * l[2]) / M_PI);
+            break;
+        }
         case 16: {
             int n = (int)lround(0.1 * g.L3);
             zc seg;
@@ -251,7 +444,8 @@ __device__ zc chi_point(double Gx0, double Gy0, double Gz0, const geo_t *geo, in
             double l[3];
             if (cell == 0) { l[0] = g0.L1; l[1] = g0.L2; l[2] = g0.L3; }
             else { l[0] = g0.SL1; l[1] = g0.SL2; l[2] = g0.SL3; }
-            if (d >= 0 && d < 3) l[d] = g.L2;
+            if (d < 0 || d > 2) break;  // another axis index leaves the prefactor alone, as in the reference
+            l[d] = g.L2;
             r *= l[0] * sinc_pi((0.5 * Gx * l[0]) / M_PI) * l[1] * sinc_pi((0.5 * Gy * l[1]) / M_PI) * l[2] *
                  sinc_pi((0.5 * Gz * l[2]) / M_PI);
             break;
@@ -316,6 +510,108 @@ __global__ void strain_kernel(const geo_t *geo, const mat_t *mat, int n_shape, c
         for (int c = 0; c < 6; c++) acc[c] += e0 * f[c];
     }
     for (int c = 0; c < 6; c++) eps[(int64_t)c * n + t] = acc[c].d2();
+}
+
+// --------------------------------------------------------------------------
+// Position-dependent elastic constants (Elastic_const 1,
+// strain_region_reciprocal_space.c:141-418, strain_fourier_coefficient.c:
+// 177-470): per shape s the initial term eps0 chi_s delta_ij, a zeroth-order
+// term with the shape's own constants, and `order` corrections, each
+// chi_s (*) (previous correction) times a factor of the constant differences
+// and the matrix's elastic Green tensor.
+// --------------------------------------------------------------------------
+__device__ double green_tensor(int comp, double Gx, double Gy, double Gz, double G, double ssum, const mat_t &p0) {
+    const int ii[6] = {0, 1, 2, 1, 0, 0}, jj[6] = {0, 1, 2, 2, 2, 1};
+    const double G3[3] = {Gx, Gy, Gz};
+    const double Gi = G3[ii[comp]], Gj = G3[jj[comp]];
+    const double D = p0.C11 - p0.C12 - 2.0 * p0.C44;
+    const double dij = ii[comp] == jj[comp] ? 1.0 : 0.0;
+    return (dij / (p0.C44 * G * G + D * Gi * Gi)) -
+           ((p0.C12 + p0.C44) * Gi * Gj /
+            ((1.0 + (p0.C12 + p0.C44) * ssum) * (p0.C44 * G * G + D * Gi * Gi) * (p0.C44 * G * G + D * Gj * Gj)));
+}
+
+__device__ double pd_order0_factor(int comp, double Gx, double Gy, double Gz, const mat_t &p0, const mat_t &ps,
+                                   int isotropic) {
+    const int ii[6] = {0, 1, 2, 1, 0, 0}, jj[6] = {0, 1, 2, 2, 2, 1};
+    const double G3[3] = {Gx, Gy, Gz};
+    const double Gi = G3[ii[comp]], Gj = G3[jj[comp]];
+    const double dij = ii[comp] == jj[comp] ? 1.0 : 0.0;
+    const double G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz);
+    const double C11 = p0.C11, C12 = p0.C12, C44 = p0.C44, D = C11 - C12 - 2.0 * C44;
+    if (fabs(G) < QD_EPS) {
+        if (isotropic == 1) return dij * (-1 * (3.0 * ps.C12 + 2.0 * ps.C44) / (3.0 * C12 + 6.0 * C44));
+        const double s0 = 1.0 / (C44 + D / 3.0);
+        return dij * ((-0.5 * (ps.C11 + 2.0 * ps.C12) / 3.0) * (2.0 / (C44 + D / 3.0)) / (1.0 + (C12 + C44) * s0));
+    }
+    if (isotropic == 1) return -((3.0 * ps.C12 + 2.0 * ps.C44) * Gi * Gj) / ((C12 + 2.0 * C44) * G * G);
+    const double ssum = (Gx * Gx) / (C44 * G * G + D * Gx * Gx) + (Gy * Gy) / (C44 * G * G + D * Gy * Gy) +
+                        (Gz * Gz) / (C44 * G * G + D * Gz * Gz);
+    return -(0.5 * (ps.C11 + 2.0 * ps.C12) * (2.0 * C44 * G * G + D * (Gi * Gi + Gj * Gj)) * Gi * Gj) /
+           ((1.0 + (C12 + C44) * ssum) * (C44 * G * G + D * Gi * Gi) * (C44 * G * G + D * Gj * Gj));
+}
+
+__device__ double pd_correction_factor(int comp, double Gx, double Gy, double Gz, const mat_t &p0, const mat_t &ps,
+                                       int isotropic) {
+    const double G = sqrt(Gx * Gx + Gy * Gy + Gz * Gz);
+    const double C11 = p0.C11, C12 = p0.C12, C44 = p0.C44, D = C11 - C12 - 2.0 * C44;
+    const double dC11 = ps.C11 - C11, dC12 = ps.C12 - C12, dC44 = ps.C44 - C44;
+    if (fabs(G) < QD_EPS) {
+        if (comp > 2) return 0.0;
+        if (isotropic == 1) return -(1.0 / (3.0 * C44)) * (ps.C11 - C11 + 2.0 * ps.C12 - 2.0 * C12);
+        const double s0 = 1.0 / (C44 + D / 3.0);
+        return -(s0 / 3.0) * (ps.C11 - C11 + 2.0 * ps.C12 - 2.0 * C12);
+    }
+    const double ssum = (Gx * Gx) / (C44 * G * G + D * Gx * Gx) + (Gy * Gy) / (C44 * G * G + D * Gy * Gy) +
+                        (Gz * Gz) / (C44 * G * G + D * Gz * Gz);
+    double g[6];
+    for (int c = 0; c < 6; c++) g[c] = green_tensor(c, Gx, Gy, Gz, G, ssum, p0);  // xx yy zz yz xz xy
+    switch (comp) {
+        case 0: return -1.0 * (Gx * ((dC11 * Gx * g[0]) + (dC12 * Gy * g[5]) + (dC12 * Gz * g[4])));
+        case 1: return -1.0 * (Gy * ((dC12 * Gx * g[5]) + (dC11 * Gy * g[1]) + (dC12 * Gz * g[3])));
+        case 2: return -1.0 * (Gz * ((dC12 * Gx * g[4]) + (dC12 * Gy * g[3]) + (dC11 * Gz * g[2])));
+        case 3: return -0.5 * dC44 * (Gy * ((Gz * g[3]) + (Gy * g[2])) + Gz * ((Gz * g[1]) + (Gy * g[3])));
+        case 4: return -0.5 * dC44 * (Gx * ((Gz * g[4]) + (Gx * g[2])) + Gz * ((Gz * g[0]) + (Gx * g[4])));
+        default: return -0.5 * dC44 * (Gx * ((Gy * g[5]) + (Gx * g[1])) + Gy * ((Gy * g[0]) + (Gx * g[5])));
+    }
+}
+
+// Initial and zeroth-order terms of shape s: eps += eps0 chi (delta + f0), corr = eps0 chi f0.
+__global__ void strain_pd_init_kernel(const geo_t *geo, const mat_t *mat, int s, const double *Gx, const double *Gy,
+                                      const double *Gz, int nx, int ny, int nz, int isotropic, const double2 *chi,
+                                      double2 *eps, double2 *corr) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int ix = (int)(t / ((int64_t)ny * nz)), iy = (int)((t / nz) % ny), iz = (int)(t % nz);
+    const double eps0 = (mat[geo[s].embedded].a - mat[s].a) / mat[0].a;
+    const zc e0 = eps0 * zc(chi[t]);
+    for (int c = 0; c < 6; c++) {
+        const zc v = e0 * pd_order0_factor(c, Gx[ix], Gy[iy], Gz[iz], mat[0], mat[s], isotropic);
+        zc acc(eps[(int64_t)c * n + t]);
+        acc += v;
+        if (c < 3) acc += e0;
+        eps[(int64_t)c * n + t] = acc.d2();
+        corr[(int64_t)c * n + t] = v.d2();
+    }
+}
+
+// One correction order of shape s from conv = chi_s (*) corr: corr = conv f_k, eps += corr.
+__global__ void strain_pd_corr_kernel(const mat_t *mat, int s, const double *Gx, const double *Gy, const double *Gz,
+                                      int nx, int ny, int nz, int isotropic, const double2 *conv, double2 *eps,
+                                      double2 *corr) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int ix = (int)(t / ((int64_t)ny * nz)), iy = (int)((t / nz) % ny), iz = (int)(t % nz);
+    for (int c = 0; c < 6; c++) {
+        const zc v = zc(conv[(int64_t)c * n + t]) * pd_correction_factor(c, Gx[ix], Gy[iy], Gz[iz], mat[0], mat[s],
+                                                                           isotropic);
+        zc acc(eps[(int64_t)c * n + t]);
+        acc += v;
+        eps[(int64_t)c * n + t] = acc.d2();
+        corr[(int64_t)c * n + t] = v.d2();
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -700,13 +996,12 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
     int ns = P.n_shape;
     cudaStream_t st = 0;
     RC(upload_gl_rule());
-    for (int s = 0; s < ns; s++) {
+    for (int s = 1; s < ns; s++) {
         int sh = pr->geo[s].shape;
-        if (s > 0 && !(sh == 0 || sh == 4 || sh == 5 || sh == 6 || sh == 16 || sh == 17))
-            return qd_set_error(QD_ERR_UNSUPPORTED, "shape %d (shape index %d) is not implemented", sh, s);
+        if (sh < 0 || sh > 18) return qd_set_error(QD_ERR_INPUT, "unknown shape %d (shape index %d)", sh, s);
     }
-    if (P.strain && P.elastic_const != 0)
-        return qd_set_error(QD_ERR_UNSUPPORTED, "position-dependent elastic constants (Elastic_const: 1)");
+    if (P.strain && P.elastic_const != 0 && P.elastic_order < 0)
+        return qd_set_error(QD_ERR_INPUT, "Elastic_const_order must be >= 0");
     if (P.strain && pr->p.strain_type == 1) {
         // 8_band_main.c:159-192: the strain grid must resolve every RL-th wave vector
         const int rl[3] = {pr->geo[0].RL1, pr->geo[0].RL2, pr->geo[0].RL3};
@@ -757,9 +1052,46 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             for (int s = 0; s < ns; s++) pr->mat[s].C44 = 0.5 * (pr->mat[s].C11 - pr->mat[s].C12);
             CK(cudaMemcpy(pr->d_mat, pr->mat, sizeof(mat_t) * ns, cudaMemcpyHostToDevice));
         }
-        strain_kernel<<<nblk(nTS, 128), 128, 0, st>>>(dg, dm, ns, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2], pr->NTS[0],
-                                                      pr->NTS[1], pr->NTS[2], P.isotropic, chi_s, eps_s);
-        CK(cudaGetLastError());
+        if (P.elastic_const == 0) {
+            strain_kernel<<<nblk(nTS, 128), 128, 0, st>>>(dg, dm, ns, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
+                                                          pr->NTS[0], pr->NTS[1], pr->NTS[2], P.isotropic, chi_s,
+                                                          eps_s);
+            CK(cudaGetLastError());
+        } else {
+            CK(cudaMemsetAsync(eps_s, 0, sizeof(double2) * nTS * 6, st));
+            Grid3 pg = {{2 * pr->NTS[0] - 1, 2 * pr->NTS[1] - 1, 2 * pr->NTS[2] - 1}};
+            const int64_t np = pg.size();
+            double2 *corr, *conv, *work;
+            RC(dalloc(&corr, sizeof(double2) * nTS * 6));
+            RC(dalloc(&conv, sizeof(double2) * nTS * 6));
+            RC(dalloc(&work, sizeof(double2) * np * 13));  // X, 6 transformed corrections, 6 products
+            double2 *X = work, *Ch = X + np, *tmp = Ch + 6 * np;
+            for (int s = 1; s < ns; s++) {
+                strain_pd_init_kernel<<<nblk(nTS, 128), 128, 0, st>>>(
+                    dg, dm, s, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2], pr->NTS[0], pr->NTS[1], pr->NTS[2],
+                    P.isotropic, chi_s + (int64_t)s * nTS, eps_s, corr);
+                if (P.elastic_order > 0) {
+                    pad_kernel<<<dim3(nblk(np, 256), 1), 256, 0, st>>>(chi_s + (int64_t)s * nTS, 0, X, 0, pr->NTS[0],
+                                                                       pr->NTS[1], pr->NTS[2], pg.n[0], pg.n[1],
+                                                                       pg.n[2]);
+                    RC(dft3(X, 0, 1, pg, -1, st));
+                }
+                for (int k = 1; k <= P.elastic_order; k++) {
+                    pad_kernel<<<dim3(nblk(np, 256), 6), 256, 0, st>>>(corr, nTS, Ch, np, pr->NTS[0], pr->NTS[1],
+                                                                       pr->NTS[2], pg.n[0], pg.n[1], pg.n[2]);
+                    RC(dft3(Ch, np, 6, pg, -1, st));
+                    RC(conv_batch(X, Ch, 6, pg, pr->NTS, tmp, conv, st));
+                    strain_pd_corr_kernel<<<nblk(nTS, 128), 128, 0, st>>>(
+                        dm, s, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2], pr->NTS[0], pr->NTS[1], pr->NTS[2], P.isotropic,
+                        conv, eps_s, corr);
+                }
+            }
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));
+            cudaFree(corr);
+            cudaFree(conv);
+            cudaFree(work);
+        }
         if (P.piezo != 0) {
             Grid3 pg = {{2 * pr->NTS[0] - 1, 2 * pr->NTS[1] - 1, 2 * pr->NTS[2] - 1}};
             int64_t np = pg.size();
