@@ -383,6 +383,9 @@ int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void *V, const 
  * launch), 1 the Hermitian rank-2K trailing update (work = 8 mt (mt+1) K
  * flops per launch).  Synchronises the device and resets the counters. */
 int qd_tc_kernel_stats(int which, long long *launches, double *ms, double *work);
+/* Per-launch device time (ms) and algorithmic work of the same kernels since the
+ * last qd_tc_kernel_stats reset (up to cap launches); returns the count. */
+int qd_tc_kernel_launches(int which, int cap, double *ms, double *work);
 
 /* Throughput (TFLOP/s) of a plain cuBLAS n^3 GEMM: kind 0 DGEMM (FP64), 1
  * SGEMM on TF32 tensor cores, 2 ZGEMM; `reps` timed launches after one

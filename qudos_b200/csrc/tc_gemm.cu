@@ -940,6 +940,7 @@ constexpr int SMEM_EXTRA = 1024 /*alignment*/ + 512 /*barriers*/;
 // X product (8 m^2), flops of the Hermitian rank-2K update (8 mt (mt+1) K).
 struct KernelTimer {
     std::vector<cudaEvent_t> ev;
+    std::vector<double> launch_work;  // algorithmic work of each timed launch
     int used = 0;
     double work = 0.0;
 };
@@ -970,6 +971,7 @@ int launch_xprod(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &
     CUDA_OK(cudaGetLastError());
     timer_mark(0, st);
     g_timer[0].work += 8.0 * (double)args.rows * (double)args.rows;
+    g_timer[0].launch_work.push_back(8.0 * (double)args.rows * (double)args.rows);
     return QD_OK;
 }
 
@@ -989,6 +991,7 @@ int launch_flush(const CUtensorMap &a, const CUtensorMap &alo, const CUtensorMap
     CUDA_OK(cudaGetLastError());
     timer_mark(1, st);
     g_timer[1].work += 8.0 * (double)args.rows * (double)(args.rows + 1) * (double)args.kdim;
+    g_timer[1].launch_work.push_back(8.0 * (double)args.rows * (double)(args.rows + 1) * (double)args.kdim);
     return QD_OK;
 }
 
@@ -1164,6 +1167,25 @@ extern "C" int qd_tc_flush(void *A, int64_t lda, int64_t off, int mt, const void
     return launch_flush(ta, talo, tb, tblo, a, st);
 }
 
+// Per-launch device times (ms) and algorithmic work of the X-product (which =
+// 0) or trailing-update kernel (which = 1) since the previous reset, without
+// resetting: up to `cap` launches into ms[] and work[]; returns the number
+// of launches recorded (or a negative QD_ERR_*).  Synchronises the device.
+extern "C" int qd_tc_kernel_launches(int which, int cap, double *ms, double *work) {
+    if (which < 0 || which > 1 || cap < 0) return -qd_set_error(QD_ERR_ARG, "qd_tc_kernel_launches: bad arguments");
+    if (cudaDeviceSynchronize() != cudaSuccess) return -qd_set_error(QD_ERR_CUDA, "qd_tc_kernel_launches: sync");
+    KernelTimer &t = g_timer[which];
+    const int n = t.used / 2;
+    for (int i = 0; i < n && i < cap; i++) {
+        float x = 0.f;
+        if (cudaEventElapsedTime(&x, t.ev[2 * i], t.ev[2 * i + 1]) != cudaSuccess)
+            return -qd_set_error(QD_ERR_CUDA, "qd_tc_kernel_launches: event");
+        ms[i] = x;
+        work[i] = i < (int)t.launch_work.size() ? t.launch_work[i] : 0.0;
+    }
+    return n;
+}
+
 // Launches, summed device time (ms) and algorithmic work of the X-product
 // (which = 0; work in bytes) or trailing-update kernel (which = 1; work in
 // flops) since the previous call; synchronises the device.
@@ -1182,5 +1204,6 @@ extern "C" int qd_tc_kernel_stats(int which, long long *launches, double *ms, do
     *work = t.work;
     t.used = 0;
     t.work = 0.0;
+    t.launch_work.clear();
     return QD_OK;
 }

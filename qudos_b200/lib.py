@@ -111,6 +111,7 @@ _sig("qd_tc_work_check", ci, [vp])
 _sig("qd_tc_xprod", ci, [vp, i64, i64, i64, ci, vp, i64, ci, vp, i64, vp, vp])
 _sig("qd_tc_flush", ci, [vp, i64, i64, ci, vp, vp, i64, i64, ci, vp, vp])
 _sig("qd_tc_kernel_stats", ci, [ci, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)])
+_sig("qd_tc_kernel_launches", ci, [ci, ci, C.POINTER(C.c_double), C.POINTER(C.c_double)])
 _sig("qd_gemm_peak", ci, [ci, ci, ci, C.POINTER(C.c_double)])
 _sig("qd_tsmm_nn", ci, [ci, ci, ci, ci, C.POINTER(vp), C.POINTER(i64), C.POINTER(vp), C.POINTER(i64), C.POINTER(ci),
                         C.POINTER(ci), C.POINTER(C.c_double), vp, i64, C.c_double, vp])

@@ -37,6 +37,8 @@ def main(argv=None):
     ap.add_argument("--solves", type=int, default=1)
     ap.add_argument("--post", action="store_true")
     ap.add_argument("--deck", choices=["molecule_15", "lens_7", "pyramid_11"], default="molecule_15")
+    ap.add_argument("--xprod-curve", action="store_true",
+                    help="print the X-product kernel's bandwidth per launch of the last solve, binned by m")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
         if a.deck == "molecule_15":
@@ -55,6 +57,11 @@ def main(argv=None):
     Z = L.DeviceBuffer(n * m * 16)
     W = L.DeviceBuffer(m * 8)
     for s in range(a.solves):
+        if s == a.solves - 1:  # per-launch timers cover the last solve only
+            import ctypes
+            cnt, ms_, wk_ = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+            for which in (0, 1):
+                L.check(L.lib.qd_tc_kernel_stats(which, ctypes.byref(cnt), ctypes.byref(ms_), ctypes.byref(wk_)))
         t0 = time.perf_counter()
         L.check(L.lib.qd_problem_assemble_dev(pr.handle, H.ptr, n, 0, q.QD_PREC_FP64, None))
         L.check(L.lib.qd_eigh_window_dev(n, H.ptr, n, lo, hi, prec, W.ptr, Z.ptr, n, None))
@@ -66,6 +73,27 @@ def main(argv=None):
         if os.environ.get("QD_PROFILE", "0") not in ("", "0"):
             pf = L.stage1_profile()
             print("    band reduction steps (ms): " + ", ".join("%s %.1f" % (k, v) for k, v in zip(STEPS, pf)))
+    if a.xprod_curve and prec == q.QD_PREC_MIXED:
+        import ctypes
+        import numpy as np
+        cap = 4 * n
+        ms = np.zeros(cap)
+        wk = np.zeros(cap)
+        k = L.lib.qd_tc_kernel_launches(0, cap, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        wk.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if k < 0:
+            L.check(-k)
+        ms, wk = ms[:k], wk[:k]
+        mm = np.sqrt(wk / 8.0)
+        print("xprod per launch (m bins: launches, total ms, GB/s):")
+        edges = [0, 2000, 5000, 10000, 15000, 20000, 25000, 10 ** 9]
+        for lo_, hi_ in zip(edges[:-1], edges[1:]):
+            sel = (mm >= lo_) & (mm < hi_)
+            if sel.any():
+                print("  m in [%d, %s): %d, %.1f ms, %.0f GB/s" %
+                      (lo_, hi_ if hi_ < 10 ** 9 else "inf", sel.sum(), ms[sel].sum(),
+                       wk[sel].sum() / (ms[sel].sum() * 1e-3) / 1e9))
+        print("  all: %d, %.1f ms, %.0f GB/s" % (k, ms.sum(), wk.sum() / (ms.sum() * 1e-3) / 1e9))
     if a.post:
         import numpy as np
         w = np.empty(m)
