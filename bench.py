@@ -305,6 +305,7 @@ def run_gpu(args, ws, rank, local):
     if not args.no_batch:
         from qudos_b200 import batch as qbatch
         batch = qbatch.measure(64, 8, 0)
+    grad = None if args.no_grad else gradients_c4()
     cpu = None
     if rank == 0 and not args.no_cpu:
         cms, pexp, (t7, n7, t9, n9) = cpu_estimate()
@@ -357,9 +358,39 @@ def run_gpu(args, ws, rank, local):
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "batch_c5": batch,
+        "gradients_c4": grad,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def gradients_c4():
+    """C4: Hellmann-Feynman gradients of the lowest 8 + 8 window states of the
+    11^3 In0.6Ga0.4As pyramid (N_H = 10648, Fz = 10 kV/cm) with respect to dot
+    height, base width, composition, field, Ep and gamma_1, after one FP64
+    solve.  Host wall time of eigen_gradients_8_band with the FFT-correlation
+    contraction (the default) and with the direct lower-triangle sum."""
+    import ctypes as C
+    import qudos_b200 as q
+    from qudos_b200 import configs, lib as L
+    params = [(L.QD_GRAD_LENGTH, 1, 4), (L.QD_GRAD_BASE, 1, 0), (L.QD_GRAD_COMPOSITION, 1, 0),
+              (L.QD_GRAD_FIELD, 0, 2), (L.QD_GRAD_EP, 0, 0), (L.QD_GRAD_GAMMA1, 0, 0)]
+    with tempfile.TemporaryDirectory() as d:
+        configs.write_deck(d, *configs.pyramid_11(mg=5, n_states=4, cme=0))
+        pr = q.Problem(d)
+        w, v = pr.solve(q.QD_PREC_FP64)
+    method = C.c_int.in_dll(L.lib, "qd_grad_method")
+    out = {"n_h": pr.n_h, "states": int(v.shape[1]), "parameters": len(params)}
+    g = {}
+    for name, m in (("fft_correlation", 0), ("direct", 1)):
+        method.value = m
+        pr.gradients(v, params)  # warm-up
+        t0 = time.perf_counter()
+        g[name] = pr.gradients(v, params)
+        out[name + "_ms"] = (time.perf_counter() - t0) * 1e3
+    method.value = 0
+    out["max_rel_diff"] = float(np.abs(g["fft_correlation"] - g["direct"]).max() / np.abs(g["direct"]).max())
+    return out
 
 
 def e2e_reference_call(pr, args, L):
@@ -394,6 +425,7 @@ def main():
     ap.add_argument("--mg", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-grad", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":

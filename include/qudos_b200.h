@@ -342,11 +342,20 @@ int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, d
  *   QD_GRAD_EP           relative scale of the binary-table Ep     per unit scale
  *   QD_GRAD_GAMMA1       relative scale of the binary-table gamma_1 per unit scale
  * H is linear in the per-difference coefficient tables, so dH/dp is the
- * Hamiltonian of dcoef/dp; that table derivative is a central difference of
- * the coefficient tables (step rel_step times the parameter's magnitude, with
- * a floor; rel_step <= 0 selects 1e-4), and the contraction with the states
- * runs on the GPU without materialising dH.  No counterpart in the reference.
- * dEdp[k * n_states + n] receives the derivative of state n for parameter k. */
+ * Hamiltonian of dcoef/dp.  For the field and the Ep and gamma_1 scales that
+ * table derivative is exact (the table is linear in the field and in the
+ * material parameters, whose derivatives are closed forms); for lengths and
+ * composition it is a central difference of two table builds (step rel_step
+ * times the parameter's magnitude, with a floor; rel_step <= 0 selects 1e-4).
+ * The contraction never forms dH: every band function is a bilinear form in
+ * G + K and G' + K, so <psi|dH|psi> = Re sum_f sum_D dcoef_f(D) C_f(D) with
+ * C_f the reciprocal-space correlations of the k-weighted envelopes, computed
+ * once per state by FFT; each parameter then costs one dot product.  No
+ * counterpart in the reference.
+ * dEdp[k * n_states + n] receives the derivative of state n for parameter k.
+ * qd_grad_method selects the contraction: 0 (default) the FFT correlations,
+ * 1 the direct sum over the lower triangle of dH (an independent check). */
+extern int qd_grad_method;
 enum {
     QD_GRAD_LENGTH = 0,
     QD_GRAD_BASE = 1,

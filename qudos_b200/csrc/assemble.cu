@@ -16,6 +16,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "qd_complex.cuh"
 #include "qd_internal.h"
 
@@ -542,5 +544,271 @@ extern "C" int qd_grad_contract(const void *d_dcoef, const double *d_Gx, const d
     cudaError_t e = cudaGetLastError();
     qd_pool_free(partial, st);
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "gradient contraction: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Hellmann-Feynman contraction as reciprocal-space correlations (the product
+// path of eigen_gradients_8_band).
+//
+// Every band function is a bilinear form in k1 = G1 + K and k2 = G2 + K whose
+// coefficients are fused-table entries at the difference G1 - G2:
+//   L_{rb,cb}(G1, G2) = sum_f coef_f(G1 - G2) sum_{a,b=0..3} M_{rb cb f a b} k1_a k2_b
+// (k_0 = 1).  With u_{b,a}(G) = k_a(G) psi_b(G) the expectation value is
+//   <psi|dH|psi> = Re sum_f sum_D dcoef_f(D) C_f(D),
+//   C_f(D) = sum_terms w c conj(u_A) (*) u_B (D) = sum_{G1 - G2 = D} ...,
+// w = 2 for the strictly lower band blocks (their upper mirror is the complex
+// conjugate) and 1 on the band diagonal.  Each correlation is an FFT product:
+// with U = FFT(u) on a grid of P >= 2N - 1 points per axis (no wrap-around of
+// D), sum_{G1 - G2 = D} conj(u_A(G1)) u_B(G2) = FFT[conj(U_A) U_B](D) / P^3, and
+// by linearity every field needs one transform of the summed spectral
+// products.  Per state: 32 forward transforms of the weighted envelopes, 28 of
+// the field spectra; then each parameter costs one dot product of its
+// derivative table with C.  dH is never formed.
+//
+// The coefficients M are read off the band functions themselves on the device
+// (unit coefficient tables, k1, k2 in {0, e_x, e_y, e_z}), so the bilinear
+// forms cannot drift from the assembly.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int GT_MAX = 1024;
+struct GradTerm {
+    int f, A, B, pad;
+    double cr, ci;
+};
+__constant__ GradTerm c_gterms[GT_MAX];
+__constant__ int c_gterm_off[QD_N_COEF + 1];
+
+// out[((f 4 + i1) 4 + i2) 13 + F]: band function F with coefficient table e_f,
+// k1 = e_{i1}, k2 = e_{i2} (index 0: the zero vector), K = 0.
+__global__ void grad_poly_kernel(const double2 *ident, double2 *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= QD_N_COEF * 16) return;
+    const int f = t / 16, i1 = (t / 4) % 4, i2 = t % 4;
+    Ctx c;
+    c.coef = ident;
+    c.nT = QD_N_COEF;
+    for (int a = 0; a < 3; a++) {
+        c.G[a] = nullptr;
+        c.N[a] = c.NT[a] = 1;
+        c.off[a] = 0;
+        c.K[a] = 0.0;
+    }
+    double g1[3] = {0.0, 0.0, 0.0}, g2[3] = {0.0, 0.0, 0.0};
+    if (i1) g1[i1 - 1] = 1.0;
+    if (i2) g2[i2 - 1] = 1.0;
+    zc v[13];
+    band_values(c, f, g1, g2, v);
+    for (int F = 0; F < 13; F++) out[t * 13 + F] = v[F].d2();
+}
+
+// U[(s 32 + b 4 + a) P^3 + g] = k_a(G) psi_s[b, G] at grid point g = G's
+// plane-wave index (ix, iy, iz) inside the P0 x P1 x P2 grid, zero elsewhere.
+__global__ void grad_weight_kernel(const double2 *psi, int64_t ldz, int m, int npw, int n0, int n1, int n2,
+                                   int p0, int p1, int p2, const double *Gx, const double *Gy, const double *Gz,
+                                   int o0, int o1, int o2, double K0, double K1, double K2, double2 *U) {
+    const int64_t P3 = (int64_t)p0 * p1 * p2;
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (g >= P3 || s >= m) return;
+    const int ix = (int)(g / ((int64_t)p1 * p2)), iy = (int)((g / p2) % p1), iz = (int)(g % p2);
+    double2 *u = U + (int64_t)s * 32 * P3 + g;
+    if (ix >= n0 || iy >= n1 || iz >= n2) {
+        for (int A = 0; A < 32; A++) u[A * P3] = make_double2(0.0, 0.0);
+        return;
+    }
+    const int pw = (ix * n1 + iy) * n2 + iz;
+    const double k[4] = {1.0, Gx[o0 + ix] + K0, Gy[o1 + iy] + K1, Gz[o2 + iz] + K2};
+    for (int b = 0; b < 8; b++) {
+        const double2 v = psi[(int64_t)s * ldz + (int64_t)b * npw + pw];
+        for (int a = 0; a < 4; a++) u[(b * 4 + a) * P3] = make_double2(k[a] * v.x, k[a] * v.y);
+    }
+}
+
+// S[(s 28 + f) P^3 + g] = sum over the terms of field f of c conj(U_A(g)) U_B(g).
+constexpr int GS_PTS = 64;
+__global__ void __launch_bounds__(GS_PTS) grad_spectral_kernel(const double2 *U, int64_t P3, int m, double2 *S) {
+    __shared__ double2 u[32][GS_PTS];
+    const int s = blockIdx.y;
+    const int64_t g = blockIdx.x * (int64_t)GS_PTS + threadIdx.x;
+    const bool ok = g < P3 && s < m;
+    for (int A = 0; A < 32; A++)
+        u[A][threadIdx.x] = ok ? U[((int64_t)s * 32 + A) * P3 + g] : make_double2(0.0, 0.0);
+    // each thread reads only its own column: no barrier needed
+    if (!ok) return;
+    for (int f = 0; f < QD_N_COEF; f++) {
+        double re = 0.0, im = 0.0;
+        for (int t = c_gterm_off[f]; t < c_gterm_off[f + 1]; t++) {
+            const GradTerm T = c_gterms[t];
+            const double2 a = u[T.A][threadIdx.x], b = u[T.B][threadIdx.x];
+            // conj(a) b
+            const double pr = a.x * b.x + a.y * b.y, pi = a.x * b.y - a.y * b.x;
+            re += T.cr * pr - T.ci * pi;
+            im += T.cr * pi + T.ci * pr;
+        }
+        S[((int64_t)s * QD_N_COEF + f) * P3 + g] = make_double2(re, im);
+    }
+}
+
+// out[s] = Re sum_f sum_t dcoef[f][t] C[s][f][D(t) mod P] / P^3; one block per state.
+__global__ void __launch_bounds__(256) grad_dot_kernel(const double2 *dcoef, int nt0, int nt1, int nt2,
+                                                       const double2 *C, int p0, int p1, int p2, double *out) {
+    __shared__ double red[8];
+    const int s = blockIdx.x;
+    const int64_t nT = (int64_t)nt0 * nt1 * nt2, P3 = (int64_t)p0 * p1 * p2;
+    double acc = 0.0;
+    for (int64_t idx = threadIdx.x; idx < QD_N_COEF * nT; idx += blockDim.x) {
+        const int f = (int)(idx / nT);
+        const int64_t t = idx - f * nT;
+        const int ix = (int)(t / ((int64_t)nt1 * nt2)), iy = (int)((t / nt2) % nt1), iz = (int)(t % nt2);
+        int dx = ix - nt0 / 2, dy = iy - nt1 / 2, dz = iz - nt2 / 2;
+        dx += dx < 0 ? p0 : 0;
+        dy += dy < 0 ? p1 : 0;
+        dz += dz < 0 ? p2 : 0;
+        const double2 a = dcoef[idx], b = C[((int64_t)s * QD_N_COEF + f) * P3 + ((int64_t)dx * p1 + dy) * p2 + dz];
+        acc += a.x * b.x - a.y * b.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        out[s] = t / (double)P3;
+    }
+}
+
+// Smallest P >= n whose prime factors are 2, 3, 5 and 7.
+int fft_size(int n) {
+    for (int p = n > 1 ? n : 1;; p++) {
+        int m = p;
+        for (int f : {2, 3, 5, 7})
+            while (m % f == 0) m /= f;
+        if (m == 1) return p;
+    }
+}
+
+int g_nterms = -1;
+
+// Term table (field, weighted envelope A, weighted envelope B, w c), once per process.
+int upload_grad_terms() {
+    if (g_nterms >= 0) return QD_OK;
+    double2 *ident = nullptr, *poly = nullptr;
+    const size_t npoly = (size_t)QD_N_COEF * 16 * 13;
+    if (cudaMalloc(&ident, sizeof(double2) * QD_N_COEF * QD_N_COEF) != cudaSuccess ||
+        cudaMalloc(&poly, sizeof(double2) * npoly) != cudaSuccess) {
+        cudaFree(ident);
+        return qd_set_error(QD_ERR_NOMEM, "gradient term extraction");
+    }
+    double2 id_h[QD_N_COEF * QD_N_COEF];
+    for (int i = 0; i < QD_N_COEF * QD_N_COEF; i++) id_h[i] = make_double2(i % (QD_N_COEF + 1) == 0 ? 1.0 : 0.0, 0.0);
+    std::vector<double2> L(npoly);
+    int rc = QD_OK;
+    if (cudaMemcpy(ident, id_h, sizeof(id_h), cudaMemcpyHostToDevice) != cudaSuccess) rc = QD_ERR_CUDA;
+    if (rc == QD_OK) {
+        qd_count_launch(1);
+        grad_poly_kernel<<<(QD_N_COEF * 16 + 127) / 128, 128>>>(ident, poly);
+        if (cudaMemcpy(L.data(), poly, sizeof(double2) * npoly, cudaMemcpyDeviceToHost) != cudaSuccess) rc = QD_ERR_CUDA;
+    }
+    cudaFree(ident);
+    cudaFree(poly);
+    if (rc) return qd_set_error(QD_ERR_CUDA, "gradient term extraction failed");
+    std::vector<GradTerm> terms;
+    int off[QD_N_COEF + 1];
+    for (int f = 0; f < QD_N_COEF; f++) {
+        off[f] = (int)terms.size();
+        for (int rb = 0; rb < 8; rb++)
+            for (int cb = 0; cb <= rb; cb++) {
+                const int F = bfunc(rb, cb);
+                if (F == F_ZERO) continue;
+                const double w = (rb > cb ? 2.0 : 1.0) * bfac(rb, cb);
+                auto val = [&](int i1, int i2) {
+                    const double2 v = L[((size_t)(f * 4 + i1) * 4 + i2) * 13 + F];
+                    return zc(v.x, v.y);
+                };
+                const zc c00 = val(0, 0);
+                for (int a = 0; a < 4; a++)
+                    for (int b = 0; b < 4; b++) {
+                        zc cab;
+                        if (a == 0 && b == 0) cab = c00;
+                        else if (b == 0) cab = val(a, 0) - c00;
+                        else if (a == 0) cab = val(0, b) - c00;
+                        else cab = val(a, b) - val(a, 0) - val(0, b) + c00;
+                        if (fabs(cab.re) + fabs(cab.im) < 1e-12) continue;
+                        GradTerm T;
+                        T.f = f;
+                        T.A = rb * 4 + a;
+                        T.B = cb * 4 + b;
+                        T.pad = 0;
+                        T.cr = w * cab.re;
+                        T.ci = w * cab.im;
+                        terms.push_back(T);
+                    }
+            }
+    }
+    off[QD_N_COEF] = (int)terms.size();
+    if ((int)terms.size() > GT_MAX) return qd_set_error(QD_ERR_UNSUPPORTED, "gradient term table: %zu terms", terms.size());
+    if (cudaMemcpyToSymbol(c_gterms, terms.data(), sizeof(GradTerm) * terms.size()) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_gterm_off, off, sizeof(off)) != cudaSuccess)
+        return qd_set_error(QD_ERR_CUDA, "gradient term upload");
+    g_nterms = (int)terms.size();
+    return QD_OK;
+}
+}  // namespace
+
+extern "C" int qd_dft3_batched(double2 *d, int64_t stride_b, int nb, const int n[3], int sign, void *stream);
+
+// Correlation tables of m states (device psi, N_H x m, ld ldz): allocates
+// *C_out = m x 28 x P^3 complex values (P from qd_grad_corr_size) on the
+// device's pool; release with qd_pool_free.
+extern "C" int qd_grad_corr_tables(const double *d_Gx, const double *d_Gy, const double *d_Gz, const int N[3],
+                                   const double K[3], const void *psi, int64_t ldz, int m, void **C_out, int P_out[3],
+                                   void *stream) {
+    if (upload_block_map() != QD_OK) return qd_set_error(QD_ERR_CUDA, "block map upload failed");
+    int rc = upload_grad_terms();
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int P[3], off[3];
+    for (int a = 0; a < 3; a++) {
+        P[a] = fft_size(2 * N[a] - 1);
+        off[a] = (2 * N[a] - 1) / 2 - N[a] / 2;
+        P_out[a] = P[a];
+    }
+    const int64_t P3 = (int64_t)P[0] * P[1] * P[2], npw = (int64_t)N[0] * N[1] * N[2];
+    double2 *U = nullptr, *S = nullptr;
+    if (qd_pool_alloc((void **)&U, sizeof(double2) * (size_t)P3 * 32 * m, st) ||
+        qd_pool_alloc((void **)&S, sizeof(double2) * (size_t)P3 * QD_N_COEF * m, st)) {
+        if (U) qd_pool_free(U, st);
+        return qd_set_error(QD_ERR_NOMEM, "gradient correlation buffers (%d states, P = %d %d %d)", m, P[0], P[1], P[2]);
+    }
+    qd_count_launch(1);
+    grad_weight_kernel<<<dim3((unsigned)((P3 + 127) / 128), (unsigned)m), 128, 0, st>>>(
+        (const double2 *)psi, ldz, m, (int)npw, N[0], N[1], N[2], P[0], P[1], P[2], d_Gx, d_Gy, d_Gz, off[0], off[1],
+        off[2], K[0], K[1], K[2], U);
+    if ((rc = qd_dft3_batched(U, P3, 32 * m, P, -1, st)) == QD_OK) {
+        qd_count_launch(1);
+        grad_spectral_kernel<<<dim3((unsigned)((P3 + GS_PTS - 1) / GS_PTS), (unsigned)m), GS_PTS, 0, st>>>(U, P3, m, S);
+        rc = qd_dft3_batched(S, P3, QD_N_COEF * m, P, -1, st);
+    }
+    cudaError_t e = cudaGetLastError();
+    qd_pool_free(U, st);
+    if (rc == QD_OK && e != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "gradient correlations: %s", cudaGetErrorString(e));
+    if (rc) {
+        qd_pool_free(S, st);
+        return rc;
+    }
+    *C_out = S;
+    return QD_OK;
+}
+
+// out[s] = <psi_s| dH |psi_s> for the derivative table d_dcoef, from the
+// correlation tables of qd_grad_corr_tables (device pointers).
+extern "C" int qd_grad_corr_dot(const void *d_dcoef, const int N[3], const void *C, const int P[3], int m,
+                                double *out_dev, void *stream) {
+    qd_count_launch(1);
+    grad_dot_kernel<<<m, 256, 0, (cudaStream_t)stream>>>((const double2 *)d_dcoef, 2 * N[0] - 1, 2 * N[1] - 1,
+                                                         2 * N[2] - 1, (const double2 *)C, P[0], P[1], P[2], out_dev);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "gradient dot: %s", cudaGetErrorString(e));
     return QD_OK;
 }

@@ -437,3 +437,47 @@ int qd_material_parameters(double T, int include_piezo, int n_shape, struct supe
     }
     return QD_OK;
 }
+
+/* Derivative of every shape's material parameters with respect to the scale
+ * of the binary table's Ep column (which = 0) or Luttinger gamma_1 column
+ * (which = 1), at the current scales.  Only sc, g1, g2, g3, Ep and P depend on
+ * them: sc_i, g1_i, g2_i, g3_i are linear in the binary Ep_i, the
+ * interpolation is linear in the binary values, and P = sqrt(HBSQM Ep / 2)
+ * gives dP = HBSQM dEp / (4 P).  Every other field of dmat is zero. */
+int qd_material_tangent(int which, int n_shape, const struct supercell_geometry *geo,
+                        const struct material_params *mat, struct material_params *dmat) {
+    double dsc[QD_N_BINARY], dg1[QD_N_BINARY], dg2[QD_N_BINARY], dEp[QD_N_BINARY];
+    for (int i = 0; i < QD_N_BINARY; i++) {
+        const double *row = qd_binary_rows[i];
+        const double Eg0 = row[C_Eg], Dso = row[C_Dso];
+        dsc[i] = dg1[i] = dg2[i] = dEp[i] = 0.0;
+        if (which == 0) {
+            dEp[i] = row[C_Ep];
+            dsc[i] = -(dEp[i] / 3.0) * (2.0 / Eg0 + 1.0 / (Eg0 + Dso));
+            dg1[i] = -dEp[i] / (3.0 * Eg0 + Dso);
+            dg2[i] = -dEp[i] / (6.0 * Eg0 + 2.0 * Dso);
+        } else {
+            dg1[i] = row[C_gL1];
+        }
+    }
+    double P[4], B[4] = {0, 0, 0, 0};
+    for (int s = 0; s < n_shape; s++) {
+        const struct supercell_geometry *g = &geo[s];
+        struct material_params *o = &dmat[s];
+        const int m = g->material, t = sys_type[m];
+        memset(o, 0, sizeof(*o));
+#define DLIN(dst, arr)                                                                            \
+    do {                                                                                          \
+        for (int q = 0; q < 4; q++) P[q] = sys_bin[m][q] >= 0 ? (arr)[sys_bin[m][q]] : 0.0;       \
+        (dst) = interp(0, t, g->x, g->y, P, B);                                                   \
+    } while (0)
+        DLIN(o->sc, dsc);
+        DLIN(o->g1, dg1);
+        DLIN(o->g2, dg2);
+        o->g3 = o->g2; /* g2 and g3 share the Ep correction and neither has a gamma_1 term */
+        DLIN(o->Ep, dEp);
+#undef DLIN
+        o->P = mat[s].P > 0.0 ? QD_HBSQM * o->Ep / (4.0 * mat[s].P) : 0.0;
+    }
+    return QD_OK;
+}

@@ -675,6 +675,20 @@ static void grad_units(int kind, double *floor_, double *to_user) {
     }
 }
 
+/* Contraction used by eigen_gradients_8_band: 0 = reciprocal-space
+ * correlations by FFT (default), 1 = the direct sum over the lower triangle of
+ * dH (an independent check). */
+int qd_grad_method = 0;
+
+int qd_material_tangent(int which, int n_shape, const struct supercell_geometry *geo,
+                        const struct material_params *mat, struct material_params *dmat);
+int qd_tables_tangent_dev(struct qd_problem *pr, const struct material_params *dmat, const double dF[3], void *dcoef);
+
+int qd_grad_corr_tables(const double *d_Gx, const double *d_Gy, const double *d_Gz, const int N[3], const double K[3],
+                        const void *psi, int64_t ldz, int m, void **C_out, int P_out[3], void *stream);
+int qd_grad_corr_dot(const void *d_dcoef, const int N[3], const void *C, const int P[3], int m, double *out_dev,
+                     void *stream);
+
 int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int n_states,
                            const qd_grad_param *params, int n_params, double rel_step, double *dEdp) {
     if (!pr || !eigvec_host || !params || !dEdp || n_states < 1 || n_params < 1)
@@ -694,39 +708,73 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
     if (rc == QD_OK && cudaMemcpy(Z, eigvec_host, sizeof(qd_complex128) * (size_t)nh * n_states,
                                   cudaMemcpyHostToDevice) != cudaSuccess)
         rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: eigenvector upload");
+    /* correlation tables of the states, shared by every parameter */
+    void *corr = NULL;
+    int P[3] = {0, 0, 0};
+    const int direct = qd_grad_method == 1;
+    if (rc == QD_OK && !direct)
+        rc = qd_grad_corr_tables(pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, Z, nh, n_states, &corr, P, NULL);
     /* originals, restored exactly after each parameter */
     const int ns = pr->p.n_shape;
     struct supercell_geometry *geo0 = (struct supercell_geometry *)malloc(sizeof(*geo0) * ns);
     qd_params p0 = pr->p;
     const double sEp = qd_scale_Ep, sg1 = qd_scale_gL1;
-    if (!geo0) rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band");
+    struct material_params *dmat = (struct material_params *)malloc(sizeof(*dmat) * ns);
+    if (!geo0 || !dmat) rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band");
     else memcpy(geo0, pr->geo, sizeof(*geo0) * ns);
-    for (int k = 0; rc == QD_OK && k < n_params; k++) {
-        const qd_grad_param *q = &params[k];
-        double v0 = 0.0, floor_ = 1.0, to_user = 1.0;
-        if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
-        grad_units(q->kind, &floor_, &to_user);
-        const double h = rel_step * (fabs(v0) > floor_ ? fabs(v0) : floor_);
-        for (int side = 0; rc == QD_OK && side < 2; side++) {
-            double dummy;
-            if ((rc = grad_apply(pr, q, side == 0 ? h : -h, &dummy))) break;
-            release_tables(pr);
-            if ((rc = qd_tables_build_dev(pr))) break;
-            if (cudaMemcpy(side == 0 ? dplus : dminus, pr->d_coef, sizeof(qd_complex128) * (size_t)ncoef,
-                           cudaMemcpyDeviceToDevice) != cudaSuccess)
-                rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: table copy");
-            /* back to the exact original values before the other side */
-            memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
-            pr->p = p0;
-            qd_scale_Ep = sEp;
-            qd_scale_gL1 = sg1;
-            if (rc == QD_OK) rc = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+    /* Two passes: first the parameters whose derivative table is exact (the
+     * table is linear in the field and in the material parameters, so it is
+     * the fused sum of the tangents, taken on the problem's own tables), then
+     * those that move the shapes or the composition (central difference of two
+     * table builds; they leave the tables rebuilt at a perturbed point). */
+    for (int pass = 0; pass < 2 && rc == QD_OK; pass++)
+        for (int k = 0; rc == QD_OK && k < n_params; k++) {
+            const qd_grad_param *q = &params[k];
+            const int exact = q->kind == QD_GRAD_FIELD || q->kind == QD_GRAD_EP || q->kind == QD_GRAD_GAMMA1;
+            if (exact != (pass == 0)) continue;
+            if (exact) {
+                double dF[3] = {0.0, 0.0, 0.0};
+                if (q->kind == QD_GRAD_FIELD) {
+                    if (q->index < 0 || q->index > 2) {
+                        rc = qd_set_error(QD_ERR_ARG, "field component %d", q->index);
+                        break;
+                    }
+                    dF[q->index] = 1.0;
+                    memset(dmat, 0, sizeof(*dmat) * ns);
+                } else if ((rc = qd_material_tangent(q->kind == QD_GRAD_EP ? 0 : 1, ns, pr->geo, pr->mat, dmat))) {
+                    break;
+                }
+                if ((rc = qd_tables_tangent_dev(pr, dmat, dF, dcoef))) break;
+            } else {
+                double v0 = 0.0, floor_ = 1.0, to_user = 1.0;
+                if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
+                grad_units(q->kind, &floor_, &to_user);
+                const double h = rel_step * (fabs(v0) > floor_ ? fabs(v0) : floor_);
+                for (int side = 0; rc == QD_OK && side < 2; side++) {
+                    double dummy;
+                    if ((rc = grad_apply(pr, q, side == 0 ? h : -h, &dummy))) break;
+                    release_tables(pr);
+                    if ((rc = qd_tables_build_dev(pr))) break;
+                    if (cudaMemcpy(side == 0 ? dplus : dminus, pr->d_coef, sizeof(qd_complex128) * (size_t)ncoef,
+                                   cudaMemcpyDeviceToDevice) != cudaSuccess)
+                        rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: table copy");
+                    /* back to the exact original values before the other side */
+                    memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
+                    pr->p = p0;
+                    qd_scale_Ep = sEp;
+                    qd_scale_gL1 = sg1;
+                    if (rc == QD_OK) rc = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+                }
+                if (rc) break;
+                if ((rc = qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL))) break;
+            }
+            if (direct)
+                rc = qd_grad_contract(dcoef, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, Z, nh, n_states,
+                                      out + (size_t)k * n_states, NULL);
+            else
+                rc = qd_grad_corr_dot(dcoef, pr->p.N, corr, P, n_states, out + (size_t)k * n_states, NULL);
         }
-        if (rc) break;
-        if ((rc = qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL))) break;
-        rc = qd_grad_contract(dcoef, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->p.N, pr->p.K, Z, nh, n_states,
-                              out + (size_t)k * n_states, NULL);
-    }
+    free(dmat);
     /* the problem's own tables again */
     if (geo0) {
         memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
@@ -748,7 +796,7 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
             for (int s = 0; s < n_states; s++) dEdp[(size_t)k * n_states + s] *= to_user;
         }
     }
-    void *bufs[] = {Z, dplus, dminus, dcoef, out};
+    void *bufs[] = {Z, dplus, dminus, dcoef, out, corr};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i]) qd_pool_free(bufs[i], NULL);
     return rc;

@@ -660,47 +660,131 @@ __global__ void mul_kernel(const double2 *a, int64_t sa, const double2 *c, int64
 
 // In-place 1-D DFT along one axis for nb arrays: X[k] = sum_j x[j] exp(sign 2 pi i j k / n).
 // One block per line; line and twiddles in shared memory.
-__global__ void dft_axis_kernel(double2 *data, int64_t stride_b, int n0, int n1, int n2, int axis, int sign) {
+// Batched 1-D FFTs along one axis of nb three-dimensional arrays: mixed-radix
+// Stockham (self-sorting) transforms in shared memory, LPB lines per block.
+// A stage of radix R over a line of n points with Ns = product of the radices
+// already applied takes, for every j < n / R, the inputs x[j + r n / R],
+// multiplies them by w^(r k) with k = j mod Ns and w = exp(sign 2 pi i /
+// (Ns R)), applies the R-point DFT and writes the results to
+// (j / Ns) Ns R + k + q Ns (q < R).  Radices 4, 2, 3, 5, 7 come first, any other
+// prime factor is one stage of an R-point DFT.  Every twiddle is a power of
+// exp(sign 2 pi i / n), tabulated once per block with sincospi.
+constexpr int FFT_MAX_STAGES = 16;
+struct FftAxis {
+    int n, nst;
+    int radix[FFT_MAX_STAGES];
+};
+
+__global__ void __launch_bounds__(128) fft_axis_kernel(double2 *data, int64_t stride_b, int n0, int n1, int n2,
+                                                       int axis, int sign, FftAxis fa, int lpb, int64_t lines) {
     extern __shared__ double2 sm[];
-    int n = axis == 0 ? n0 : axis == 1 ? n1 : n2;
-    double2 *line = sm, *tw = sm + n;
-    int64_t L = blockIdx.x;
-    int b = blockIdx.y;
-    int64_t base, step;
-    if (axis == 2) { base = L * n2; step = 1; }
-    else if (axis == 1) { int i0 = (int)(L / n2), i2 = (int)(L % n2); base = (int64_t)i0 * n1 * n2 + i2; step = n2; }
-    else { base = L; step = (int64_t)n1 * n2; }
-    double2 *p = data + b * stride_b + base;
+    const int n = fa.n;
+    double2 *buf0 = sm, *buf1 = sm + lpb * n, *tw = sm + 2 * lpb * n;
+    const int64_t L0 = (int64_t)blockIdx.x * lpb;
+    const int nl = (int)min((int64_t)lpb, lines - L0);
+    double2 *p = data + (int64_t)blockIdx.y * stride_b;
+    // line L starts at base(L) and advances by step
+    int64_t step;
+    if (axis == 2) step = 1;
+    else if (axis == 1) step = n2;
+    else step = (int64_t)n1 * n2;
+    auto base = [&](int64_t L) -> int64_t {
+        if (axis == 2) return L * n2;
+        if (axis == 1) return (L / n2) * (int64_t)n1 * n2 + (L % n2);
+        return L;
+    };
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        line[j] = p[j * step];
         double s, c;
         sincospi((2.0 * j) / n, &s, &c);
         tw[j] = make_double2(c, sign * s);
     }
+    // coalesced loads: along the line for axis 2, across neighbouring lines otherwise
+    for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+        int l, e;
+        if (axis == 2) { l = idx / n; e = idx % n; }
+        else { e = idx / nl; l = idx % nl; }
+        buf0[l * n + e] = p[base(L0 + l) + e * step];
+    }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int j = 0; j < n; j++) {
-            double2 x = line[j], w = tw[idx];
-            re += x.x * w.x - x.y * w.y;
-            im += x.x * w.y + x.y * w.x;
-            idx += k;
-            if (idx >= n) idx -= n;
+    double2 *src = buf0, *dst = buf1;
+    int Ns = 1;
+    for (int st = 0; st < fa.nst; st++) {
+        const int R = fa.radix[st], nR = n / R, tstep = n / (Ns * R), dstep = nR;  // w_n^(tstep) = w_(Ns R)
+        for (int idx = threadIdx.x; idx < nl * nR; idx += blockDim.x) {
+            const int l = idx / nR, j = idx % nR, k = j % Ns;
+            const double2 *x = src + l * n;
+            double2 *y = dst + l * n + (j / Ns) * Ns * R + k;
+            for (int q = 0; q < R; q++) {
+                double re = 0.0, im = 0.0;
+                for (int r = 0; r < R; r++) {
+                    double2 v = x[j + r * nR];
+                    // twiddle w_(Ns R)^(r k) times the DFT factor w_R^(r q), as one power of w_n
+                    const int e = (int)(((int64_t)r * k * tstep + (int64_t)r * q * dstep) % n);
+                    const double2 w = tw[e];
+                    re += v.x * w.x - v.y * w.y;
+                    im += v.x * w.y + v.y * w.x;
+                }
+                y[q * Ns] = make_double2(re, im);
+            }
         }
-        p[k * step] = make_double2(re, im);
+        __syncthreads();
+        double2 *t = src;
+        src = dst;
+        dst = t;
+        Ns *= R;
+    }
+    for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+        int l, e;
+        if (axis == 2) { l = idx / n; e = idx % n; }
+        else { e = idx / nl; l = idx % nl; }
+        p[base(L0 + l) + e * step] = src[l * n + e];
     }
 }
 
+static FftAxis fft_plan(int n) {
+    FftAxis f;
+    f.n = n;
+    f.nst = 0;
+    int m = n;
+    const int small[5] = {4, 2, 3, 5, 7};
+    for (int i = 0; i < 5; i++)
+        while (m % small[i] == 0 && f.nst < FFT_MAX_STAGES - 1) {
+            f.radix[f.nst++] = small[i];
+            m /= small[i];
+        }
+    for (int pf = 11; m > 1 && f.nst < FFT_MAX_STAGES; pf += 2)
+        while (m % pf == 0) {
+            f.radix[f.nst++] = pf;
+            m /= pf;
+        }
+    if (m > 1) f.radix[f.nst++] = m;  // not reached for n < 11^16
+    return f;
+}
+
 static int dft3(double2 *d, int64_t stride_b, int nb, const Grid3 &g, int sign, cudaStream_t st) {
-    qd_count_launch(3);
+    static bool configured = false;
+    if (!configured) {
+        CK(cudaFuncSetAttribute(fft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured = true;
+    }
     for (int axis = 2; axis >= 0; axis--) {
-        int n = g.n[axis];
-        int64_t lines = g.size() / n;
-        dim3 grid((unsigned)lines, nb);
-        int threads = n < 128 ? ((n + 31) / 32) * 32 : 128;
-        dft_axis_kernel<<<grid, threads, 2 * n * sizeof(double2), st>>>(d, stride_b, g.n[0], g.n[1], g.n[2], axis,
-                                                                        sign);
+        const int n = g.n[axis];
+        if (n == 1) continue;
+        if (3 * (size_t)n * sizeof(double2) > 200 * 1024)
+            return qd_set_error(QD_ERR_UNSUPPORTED, "FFT length %d exceeds the shared-memory line buffer", n);
+        const FftAxis fa = fft_plan(n);
+        int lpb = 512 / n;
+        lpb = lpb < 1 ? 1 : lpb > 16 ? 16 : lpb;
+        while (lpb > 1 && (size_t)(2 * lpb + 1) * n * sizeof(double2) > 48 * 1024) lpb--;
+        const int64_t lines = g.size() / n;
+        const size_t smem = (size_t)(2 * lpb + 1) * n * sizeof(double2);
+        for (int b0 = 0; b0 < nb; b0 += 65535) {
+            const int bn = nb - b0 < 65535 ? nb - b0 : 65535;
+            dim3 grid((unsigned)((lines + lpb - 1) / lpb), (unsigned)bn);
+            qd_count_launch(1);
+            fft_axis_kernel<<<grid, 128, smem, st>>>(d + (int64_t)b0 * stride_b, stride_b, g.n[0], g.n[1], g.n[2],
+                                                     axis, sign, fa, lpb, lines);
+        }
     }
     CK(cudaGetLastError());
     return QD_OK;
@@ -1254,6 +1338,37 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     pr->tables_ready = 1;
+    return QD_OK;
+}
+
+// Derivative of the fused coefficient table along a direction in which the
+// shape functions, the strain and the piezoelectric potential stay fixed and
+// only the material parameters (dmat, one entry per shape) and the field (dF)
+// move.  The table is linear in both, so the derivative is the same fused sum
+// evaluated with dmat and dF in place of the parameters and field, without the
+// piezoelectric potential (it depends on neither).  Exact: Ep and gamma_1
+// scales and the field components use it.  dcoef: QD_N_COEF x nT, device.
+extern "C" int qd_tables_tangent_dev(struct qd_problem *pr, const struct material_params *dmat, const double dF[3],
+                                     void *dcoef) {
+    if (!pr->tables_ready) return qd_set_error(QD_ERR_ARG, "qd_tables_tangent_dev: tables not built");
+    const qd_params &P = pr->p;
+    const int ns = P.n_shape;
+    mat_t *dm = nullptr;
+    RC(dalloc(&dm, sizeof(mat_t) * ns));
+    cudaError_t e = cudaMemcpy(dm, dmat, sizeof(mat_t) * ns, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const geo_t &g0 = pr->geo[0];
+        qd_count_launch(1);
+        fused_coef_kernel<<<nblk(pr->nT, 128), 128>>>(
+            (const geo_t *)pr->d_geo, dm, ns, pr->NT[0], pr->NT[1], pr->NT[2], 2.0 * M_PI / g0.L1,
+            2.0 * M_PI / g0.L2, 2.0 * M_PI / g0.L3, dF[0], dF[1], dF[2], P.strain != 0, 0,
+            (const double2 *)pr->d_chi, (const double2 *)pr->d_eps, nullptr, (const double2 *)pr->d_conv,
+            (double2 *)dcoef);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    cudaFree(dm);
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "tangent table: %s", cudaGetErrorString(e));
     return QD_OK;
 }
 

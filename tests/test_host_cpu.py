@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in sorted(names) if not hasattr(L.lib, n)]
     assert not missing, missing
     for g in ("N_H", "na_rows", "characteristic_function_G", "strain_G", "convolutions_char_strain",
-              "phi_piezo_G", "include_strain", "include_piezo", "component_run_times"):
+              "phi_piezo_G", "include_strain", "include_piezo", "component_run_times", "qd_grad_method"):
         ctypes.c_int.in_dll(L.lib, g)  # global exported
 
 
