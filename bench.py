@@ -306,6 +306,7 @@ def run_gpu(args, ws, rank, local):
         from qudos_b200 import batch as qbatch
         batch = qbatch.measure(64, 8, 0)
     grad = None if args.no_grad else gradients_c4()
+    cme = None if args.no_grad else coulomb_c2()
     cpu = None
     if rank == 0 and not args.no_cpu:
         cms, pexp, (t7, n7, t9, n9) = cpu_estimate()
@@ -359,6 +360,7 @@ def run_gpu(args, ws, rank, local):
         "clocks": clk.summary(),
         "batch_c5": batch,
         "gradients_c4": grad,
+        "coulomb_c2": cme,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -368,8 +370,9 @@ def gradients_c4():
     """C4: Hellmann-Feynman gradients of the lowest 8 + 8 window states of the
     11^3 In0.6Ga0.4As pyramid (N_H = 10648, Fz = 10 kV/cm) with respect to dot
     height, base width, composition, field, Ep and gamma_1, after one FP64
-    solve.  Host wall time of eigen_gradients_8_band with the FFT-correlation
-    contraction (the default) and with the direct lower-triangle sum."""
+    solve.  Host wall time of eigen_gradients_8_band (the fastest of three
+    calls, alternating) with the FFT-correlation contraction (the default) and
+    with the direct lower-triangle sum."""
     import ctypes as C
     import qudos_b200 as q
     from qudos_b200 import configs, lib as L
@@ -381,16 +384,42 @@ def gradients_c4():
         w, v = pr.solve(q.QD_PREC_FP64)
     method = C.c_int.in_dll(L.lib, "qd_grad_method")
     out = {"n_h": pr.n_h, "states": int(v.shape[1]), "parameters": len(params)}
-    g = {}
+    g, best = {}, {}
     for name, m in (("fft_correlation", 0), ("direct", 1)):
         method.value = m
         pr.gradients(v, params)  # warm-up
-        t0 = time.perf_counter()
-        g[name] = pr.gradients(v, params)
-        out[name + "_ms"] = (time.perf_counter() - t0) * 1e3
+    for rep in range(3):  # alternating, the fastest of three calls each
+        for name, m in (("fft_correlation", 0), ("direct", 1)):
+            method.value = m
+            t0 = time.perf_counter()
+            g[name] = pr.gradients(v, params)
+            best[name] = min(best.get(name, 1e30), (time.perf_counter() - t0) * 1e3)
     method.value = 0
+    for name in best:
+        out[name + "_ms"] = best[name]
     out["max_rel_diff"] = float(np.abs(g["fft_correlation"] - g["direct"]).max() / np.abs(g["direct"]).max())
     return out
+
+
+def coulomb_c2():
+    """C2: the 11^3 In0.6Ga0.4As pyramid (N_H = 10648, Fz = 10 kV/cm, CME 1),
+    16 e + 16 h states from one FP64 solve, then the Coulomb direct and
+    exchange elements among the lowest 4 e and 4 h states (the deck's Coulomb
+    cell, densities on the 2x-oversampled 22^3 grid by FFT).  Host wall time
+    of the warm call, after one call that pays the one-time costs."""
+    import qudos_b200 as q
+    from qudos_b200 import configs
+    with tempfile.TemporaryDirectory() as d:
+        configs.write_deck(d, *configs.pyramid_11(mg=5, n_states=8, cme=1))
+        pr = q.Problem(d)
+        w, v = pr.solve(q.QD_PREC_FP64)
+    nv = 2 * pr.n_vb
+    sub = np.asfortranarray(np.concatenate([v[:, nv - 4:nv], v[:, nv:nv + 4]], axis=1))
+    pr.coulomb(sub, 4, 4, 1)
+    t0 = time.perf_counter()
+    V = pr.coulomb(sub, 4, 4, 1)
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"n_h": pr.n_h, "states": 8, "elements": int(sum(x.size for x in V.values())), "ms": ms}
 
 
 def e2e_reference_call(pr, args, L):

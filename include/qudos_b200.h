@@ -332,6 +332,15 @@ int qd_stage1_profile(double *ms, int n);
 int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, double *const *eigval,
                         qd_complex128 *const *eigvec);
 
+/* Tuning table of the dense->band reduction: for solves of order <= n_h_max
+ * in precision prec, aggregate `agg` columns (a multiple of 32, 32..256) of
+ * Householder panels before each rank-2K trailing update.  The entry with the
+ * smallest bound >= N_H applies; without one, the environment's QD_AGG or 256.
+ * n_h_max <= 0 clears the table.  Set it before the solves that should use it;
+ * the Python package fills it from the cache its autotuner writes
+ * (qudos_b200/autotune.py).  No counterpart in the reference. */
+int qd_tuning_set(int prec, int64_t n_h_max, int agg);
+
 /* Hellmann-Feynman gradients dE_n/dp = <psi_n| dH/dp |psi_n> of the states in
  * eigvec_host (N_H x n_states, host, normalised eigenvectors of the problem's
  * H) with respect to the parameters in params:

@@ -650,14 +650,18 @@ __global__ void __launch_bounds__(GS_PTS) grad_spectral_kernel(const double2 *U,
     }
 }
 
-// out[s] = Re sum_f sum_t dcoef[f][t] C[s][f][D(t) mod P] / P^3; one block per state.
+// partial[s][c] = Re sum over slice c of (f, t) of dcoef[f][t] C[s][f][D(t) mod P];
+// grid (GD_CHUNKS, states).  grad_dot_sum_kernel adds the slices of each state
+// in a fixed order, so the result does not depend on scheduling.
+constexpr int GD_CHUNKS = 64;
 __global__ void __launch_bounds__(256) grad_dot_kernel(const double2 *dcoef, int nt0, int nt1, int nt2,
-                                                       const double2 *C, int p0, int p1, int p2, double *out) {
+                                                       const double2 *C, int p0, int p1, int p2, double *partial) {
     __shared__ double red[8];
-    const int s = blockIdx.x;
-    const int64_t nT = (int64_t)nt0 * nt1 * nt2, P3 = (int64_t)p0 * p1 * p2;
+    const int s = blockIdx.y, c = blockIdx.x;
+    const int64_t nT = (int64_t)nt0 * nt1 * nt2, P3 = (int64_t)p0 * p1 * p2, tot = QD_N_COEF * nT;
+    const int64_t i0 = tot * c / GD_CHUNKS, i1 = tot * (c + 1) / GD_CHUNKS;
     double acc = 0.0;
-    for (int64_t idx = threadIdx.x; idx < QD_N_COEF * nT; idx += blockDim.x) {
+    for (int64_t idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
         const int f = (int)(idx / nT);
         const int64_t t = idx - f * nT;
         const int ix = (int)(t / ((int64_t)nt1 * nt2)), iy = (int)((t / nt2) % nt1), iz = (int)(t % nt2);
@@ -674,8 +678,17 @@ __global__ void __launch_bounds__(256) grad_dot_kernel(const double2 *dcoef, int
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
-        out[s] = t / (double)P3;
+        partial[(int64_t)s * GD_CHUNKS + c] = t;
     }
+}
+
+// out[s] = sum_c partial[s][c] / P^3, one warp per state
+__global__ void grad_dot_sum_kernel(const double *partial, int m, double inv_p3, double *out) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (s >= m) return;
+    double x = partial[(int64_t)s * GD_CHUNKS + lane] + partial[(int64_t)s * GD_CHUNKS + 32 + lane];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) out[s] = x * inv_p3;
 }
 
 // Smallest P >= n whose prime factors are 2, 3, 5 and 7.
@@ -805,9 +818,18 @@ extern "C" int qd_grad_corr_tables(const double *d_Gx, const double *d_Gy, const
 // correlation tables of qd_grad_corr_tables (device pointers).
 extern "C" int qd_grad_corr_dot(const void *d_dcoef, const int N[3], const void *C, const int P[3], int m,
                                 double *out_dev, void *stream) {
-    qd_count_launch(1);
-    grad_dot_kernel<<<m, 256, 0, (cudaStream_t)stream>>>((const double2 *)d_dcoef, 2 * N[0] - 1, 2 * N[1] - 1,
-                                                         2 * N[2] - 1, (const double2 *)C, P[0], P[1], P[2], out_dev);
+    static_assert(GD_CHUNKS == 64, "grad_dot_sum_kernel adds two slices per lane");
+    cudaStream_t st = (cudaStream_t)stream;
+    double *partial = nullptr;
+    if (qd_pool_alloc((void **)&partial, sizeof(double) * GD_CHUNKS * (size_t)m, st))
+        return qd_set_error(QD_ERR_NOMEM, "gradient dot partial sums");
+    qd_count_launch(2);
+    grad_dot_kernel<<<dim3(GD_CHUNKS, (unsigned)m), 256, 0, st>>>((const double2 *)d_dcoef, 2 * N[0] - 1,
+                                                                  2 * N[1] - 1, 2 * N[2] - 1, (const double2 *)C,
+                                                                  P[0], P[1], P[2], partial);
+    const double inv_p3 = 1.0 / ((double)P[0] * P[1] * P[2]);
+    grad_dot_sum_kernel<<<(m + 7) / 8, 256, 0, st>>>(partial, m, inv_p3, out_dev);
+    qd_pool_free(partial, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "gradient dot: %s", cudaGetErrorString(e));
     return QD_OK;

@@ -621,11 +621,57 @@ static int stage1(T *A, int64_t n, int64_t lda, int b, Stage1Work &w, cudaStream
     return QD_OK;
 }
 
+// Tuning table of the aggregation depth (columns of the rank-2K update per
+// flush), per element size (8: mixed path, 16: FP64) and matrix-size bound;
+// written by qd_tuning_set (the package's autotuner fills it from its cache).
+namespace {
+constexpr int TUNE_MAX = 64;
+struct TuneEntry {
+    int64_t n_max;
+    int elem_bytes, agg;
+};
+TuneEntry g_tune[TUNE_MAX];
+int g_ntune = 0;
+}  // namespace
+
+// Adds (or replaces) the aggregation depth for matrices of order <= n_h_max
+// solved in precision prec; n_h_max <= 0 clears the table.  Call before the
+// solves that should use it (the table is read when a solve sets up).
+extern "C" int qd_tuning_set(int prec, int64_t n_h_max, int agg) {
+    if (n_h_max <= 0) {
+        g_ntune = 0;
+        return QD_OK;
+    }
+    if (prec != QD_PREC_FP64 && prec != QD_PREC_MIXED) return qd_set_error(QD_ERR_ARG, "qd_tuning_set: precision");
+    if (agg < 32 || agg > 256 || agg % 32) return qd_set_error(QD_ERR_ARG, "qd_tuning_set: depth %d (32..256, multiple of 32)", agg);
+    const int eb = prec == QD_PREC_MIXED ? 8 : 16;
+    for (int i = 0; i < g_ntune; i++)
+        if (g_tune[i].n_max == n_h_max && g_tune[i].elem_bytes == eb) {
+            g_tune[i].agg = agg;
+            return QD_OK;
+        }
+    if (g_ntune == TUNE_MAX) return qd_set_error(QD_ERR_ARG, "qd_tuning_set: table full");
+    g_tune[g_ntune++] = {n_h_max, eb, agg};
+    return QD_OK;
+}
+
+// Depth for an order-n solve: the entry with the smallest bound >= n, else
+// QD_AGG from the environment, else 256.
+static int tuned_agg(int64_t n, int elem_bytes) {
+    int best = -1;
+    for (int i = 0; i < g_ntune; i++)
+        if (g_tune[i].elem_bytes == elem_bytes && g_tune[i].n_max >= n &&
+            (best < 0 || g_tune[i].n_max < g_tune[best].n_max))
+            best = i;
+    if (best >= 0) return g_tune[best].agg;
+    const char *s = getenv("QD_AGG");
+    return s ? atoi(s) : 256;
+}
+
 extern "C" int qd_stage1_alloc(int64_t n, int b, int elem_bytes, Stage1Work *w, cudaStream_t st) {
     w->tc = nullptr;
     w->npanels = n_panels(n, b);
-    const char *s = getenv("QD_AGG");
-    int agg = s ? atoi(s) : 256;
+    int agg = tuned_agg(n, elem_bytes);
     if (agg < b) agg = b;
     agg = (agg / b) * b;
     w->agg = agg;

@@ -715,14 +715,16 @@ __global__ void __launch_bounds__(128) fft_axis_kernel(double2 *data, int64_t st
             const double2 *x = src + l * n;
             double2 *y = dst + l * n + (j / Ns) * Ns * R + k;
             for (int q = 0; q < R; q++) {
+                // twiddle w_(Ns R)^(r k) times the DFT factor w_R^(r q) is w_n^(r inc), inc = k tstep + q dstep
+                const int inc = (int)(((int64_t)k * tstep + (int64_t)q * dstep) % n);
                 double re = 0.0, im = 0.0;
+                int e = 0;
                 for (int r = 0; r < R; r++) {
-                    double2 v = x[j + r * nR];
-                    // twiddle w_(Ns R)^(r k) times the DFT factor w_R^(r q), as one power of w_n
-                    const int e = (int)(((int64_t)r * k * tstep + (int64_t)r * q * dstep) % n);
-                    const double2 w = tw[e];
+                    const double2 v = x[j + r * nR], w = tw[e];
                     re += v.x * w.x - v.y * w.y;
                     im += v.x * w.y + v.y * w.x;
+                    e += inc;
+                    if (e >= n) e -= n;
                 }
                 y[q * Ns] = make_double2(re, im);
             }
@@ -738,6 +740,16 @@ __global__ void __launch_bounds__(128) fft_axis_kernel(double2 *data, int64_t st
         if (axis == 2) { l = idx / n; e = idx % n; }
         else { e = idx / nl; l = idx % nl; }
         p[base(L0 + l) + e * step] = src[l * n + e];
+    }
+}
+
+// Smallest size >= n whose prime factors are 2, 3, 5 and 7.
+static int smooth_size(int n) {
+    for (int p = n > 1 ? n : 1;; p++) {
+        int m = p;
+        for (int f : {2, 3, 5, 7})
+            while (m % f == 0) m /= f;
+        if (m == 1) return p;
     }
 }
 
@@ -1143,7 +1155,10 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             CK(cudaGetLastError());
         } else {
             CK(cudaMemsetAsync(eps_s, 0, sizeof(double2) * nTS * 6, st));
-            Grid3 pg = {{2 * pr->NTS[0] - 1, 2 * pr->NTS[1] - 1, 2 * pr->NTS[2] - 1}};
+            // any size >= 2 N_TS - 1 keeps the linear convolutions free of wrap-around (the crop reads
+            // the central block); the next size with factors 2, 3, 5, 7 keeps the FFTs to small radices
+            Grid3 pg = {{smooth_size(2 * pr->NTS[0] - 1), smooth_size(2 * pr->NTS[1] - 1),
+                         smooth_size(2 * pr->NTS[2] - 1)}};
             const int64_t np = pg.size();
             double2 *corr, *conv, *work;
             RC(dalloc(&corr, sizeof(double2) * nTS * 6));
@@ -1177,7 +1192,8 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             cudaFree(work);
         }
         if (P.piezo != 0) {
-            Grid3 pg = {{2 * pr->NTS[0] - 1, 2 * pr->NTS[1] - 1, 2 * pr->NTS[2] - 1}};
+            Grid3 pg = {{smooth_size(2 * pr->NTS[0] - 1), smooth_size(2 * pr->NTS[1] - 1),
+                         smooth_size(2 * pr->NTS[2] - 1)}};
             int64_t np = pg.size();
             int second = (P.piezo == 2 || P.piezo == 3);
             int nbuf = 6 + (second ? 12 : 0) + 1 + 12;
@@ -1300,7 +1316,7 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
         }
         pr->d_eps = eps; pr->d_phi = phi;
         // convolutions chi_s (*) eps_ij (convolutions.c)
-        Grid3 pg = {{2 * pr->NT[0] - 1, 2 * pr->NT[1] - 1, 2 * pr->NT[2] - 1}};
+        Grid3 pg = {{smooth_size(2 * pr->NT[0] - 1), smooth_size(2 * pr->NT[1] - 1), smooth_size(2 * pr->NT[2] - 1)}};
         int64_t np = pg.size();
         RC(dalloc(&conv, sizeof(double2) * nT * 8 * ns));
         CK(cudaMemset(conv, 0, sizeof(double2) * nT * 8 * ns));

@@ -119,6 +119,7 @@ _sig("qd_tsmm_cn", ci, [ci, ci, vp, i64, ci, vp, i64, ci, vp, i64, vp, C.c_size_
 _sig("qd_small_cn", ci, [ci, ci, ci, ci, vp, ci, vp, ci, C.c_double, vp, ci, vp])
 _sig("qd_tsmm_cn_scratch_bytes", C.c_size_t, [ci, ci, ci, ci])
 _sig("qd_set_wait_limits", ci, [C.c_longlong, C.c_longlong, C.c_longlong])
+_sig("qd_tuning_set", ci, [ci, C.c_int64, ci])
 _sig("qd_hemm_lower_dev", ci, [i64, vp, i64, vp, i64, ci, vp, i64, C.c_double, vp])
 _sig("qd_gram_dev", ci, [i64, vp, i64, ci, vp, i64, ci, vp, ci, vp])
 _sig("qd_zgemm_small_dev", ci, [i64, vp, i64, ci, vp, ci, ci, vp, i64, C.c_double, vp])

@@ -18,7 +18,13 @@ TABLE_CHI, TABLE_STRAIN, TABLE_PHI, TABLE_CONV, TABLE_CHI_S, TABLE_STRAIN_S, TAB
 
 
 class Problem:
-    def __init__(self, directory, overrides=()):
+    def __init__(self, directory, overrides=(), tuned=True):
+        """Loads parameters.in / supercell.in from directory.  tuned: put the
+        package's autotuner cache into the library's tuning table (once per
+        process) before the first solve."""
+        if tuned:
+            from . import autotune
+            autotune.ensure_loaded()
         self._h = C.c_void_p()
         arr = (C.c_char_p * max(1, len(overrides)))(*[o.encode() for o in overrides])
         L.check(L.lib.qd_problem_load(os.fsencode(directory), arr, len(overrides), C.byref(self._h)))

@@ -116,3 +116,22 @@ def test_reference_arm_loads_no_native_code():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     assert out.stdout.split() == ["0", "0"]
+
+
+def test_tuning_table_and_cache(tmp_path):
+    """The autotuner's cache goes into the library's tuning table; depths
+    outside 32..256 or not multiples of 32 are rejected."""
+    import json
+    from qudos_b200 import autotune
+    path = tmp_path / "tuning.json"
+    path.write_text(json.dumps({"entries": [{"n_h": 2744, "prec": "mixed", "depth": 128},
+                                            {"n_h": 27000, "prec": "mixed", "depth": 256},
+                                            {"n_h": 27000, "prec": "fp64", "depth": 192}]}))
+    try:
+        assert autotune.load(str(path)) == 3
+        assert L.lib.qd_tuning_set(L.QD_PREC_MIXED, 1000, 300) == L.QD_ERR_ARG
+        assert L.lib.qd_tuning_set(L.QD_PREC_MIXED, 1000, 100) == L.QD_ERR_ARG
+        assert L.lib.qd_tuning_set(7, 1000, 128) == L.QD_ERR_ARG
+        assert autotune.load(str(tmp_path / "absent.json")) == 0
+    finally:
+        autotune.load()
