@@ -89,6 +89,90 @@ __global__ void coulomb_pair_kernel(const double2 *Fa, const double2 *Fc, int64_
     }
 }
 
+// The same products with the operands staged by the TMA engine: one block takes
+// a tile of tm grid points (tm divides 256) of every state's eight band arrays of Fa
+// and Fc, brought into shared memory by bulk copies (cp.async.bulk, completion
+// counted on one mbarrier), and forms every pair from there, so each array is
+// read from memory once instead of once per pair containing its state
+// ((M + 1) / 2 times less traffic).  Threads: tm points x 256 / tm pair groups.  The
+// wait for the copies is bounded (2 s of %globaltimer); on expiry the block
+// records QD_ERR_TIMEOUT in *err, waits (bounded) for its copies and returns.
+__device__ __forceinline__ uint32_t cp_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool cp_bar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(cp_smem(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long cp_now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool cp_bar_wait(uint64_t *bar, uint32_t parity, unsigned long long limit_ns) {
+    const unsigned long long t0 = cp_now();
+    for (uint32_t it = 0;; it++) {
+        if (cp_bar_try(bar, parity)) return true;
+        if ((it & 63) == 63 && cp_now() - t0 > limit_ns) return false;
+    }
+}
+
+__global__ void __launch_bounds__(256) coulomb_pair_tma_kernel(const double2 *Fa, const double2 *Fc, int64_t S, int M,
+                                                               int tm, const int2 *pairs, int P, double2 *Bp,
+                                                               int *err) {
+    extern __shared__ __align__(128) double2 stile[];  // [2][M * 8][tm]: Fa tiles, then Fc tiles
+    __shared__ __align__(8) uint64_t bar;
+    const int nk = M * QD_N_BAND;
+    double2 *sa = stile, *sc = stile + (size_t)nk * tm;
+    const int64_t m0 = (int64_t)blockIdx.x * tm;
+    const int cnt = (int)(S - m0 < tm ? S - m0 : tm);
+    const uint32_t bytes = (uint32_t)cnt * 16u;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(cp_smem(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // warp 0 issues the copies, each lane arriving once with its own byte count
+        const int k0 = threadIdx.x;
+        const uint32_t mine = (uint32_t)((nk - k0 + 31) / 32) * 2u * bytes;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cp_smem(&bar)), "r"(mine)
+                     : "memory");
+        for (int k = k0; k < nk; k += 32) {
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    cp_smem(sa + (size_t)k * tm)),
+                "l"(Fa + (int64_t)k * S + m0), "r"(bytes), "r"(cp_smem(&bar))
+                : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    cp_smem(sc + (size_t)k * tm)),
+                "l"(Fc + (int64_t)k * S + m0), "r"(bytes), "r"(cp_smem(&bar))
+                : "memory");
+        }
+    }
+    if (!cp_bar_wait(&bar, 0, 2000000000ull)) {
+        if (threadIdx.x == 0) atomicExch(err, QD_ERR_TIMEOUT);
+        cp_bar_wait(&bar, 0, 2000000000ull);  // the copies land before the block leaves
+        return;
+    }
+    const int t = threadIdx.x % tm, g = threadIdx.x / tm, ng = blockDim.x / tm;
+    if (t >= cnt) return;
+    for (int p = g; p < P; p += ng) {
+        const int2 ij = pairs[p];
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int b = 0; b < QD_N_BAND; b++) {
+            const double2 u = sc[(size_t)(ij.x * QD_N_BAND + b) * tm + t], v = sa[(size_t)(ij.y * QD_N_BAND + b) * tm + t];
+            re += u.x * v.x - u.y * v.y;
+            im += u.x * v.y + u.y * v.x;
+        }
+        Bp[(int64_t)p * S + m0 + t] = make_double2(re, im);
+    }
+}
+
 // Same cells: B_C = (((inv_vol * B / S) * L1) * L2) * L3, the reference's order of operations.
 __global__ void coulomb_copy_kernel(const double2 *Bp, int64_t S, int P, double inv_S, double inv_vol, double L1,
                                     double L2, double L3, double2 *BC) {
@@ -277,6 +361,7 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
     double2 *V4 = nullptr, *U = nullptr, *Cc = nullptr, *Dm = nullptr, *Dc = nullptr;
     double *wd = nullptr, *Wd = nullptr;
     int2 *pairs_d = nullptr;
+    int *errd = nullptr;
     // intermediate grids of the separable Coulomb-cell transform stay within this many points
     const int64_t Smax = (int64_t)(sz3[0] > szC[0] ? sz3[0] : szC[0]) * (sz3[1] > szC[1] ? sz3[1] : szC[1]) *
                          (sz3[2] > szC[2] ? sz3[2] : szC[2]);
@@ -299,7 +384,8 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
         (rc = alloc((void **)&V4, zsz * SC * 4)) || (rc = alloc((void **)&U, zsz * P * P)) ||
         (rc = alloc((void **)&Cc, zsz * P * P)) || (rc = alloc((void **)&Dm, zsz * P * 4)) ||
         (rc = alloc((void **)&Dc, zsz * P * 4)) || (rc = alloc((void **)&wd, sizeof(double) * SC)) ||
-        (rc = alloc((void **)&Wd, sizeof(double) * 3 * 128 * 128)) || (rc = alloc((void **)&pairs_d, sizeof(int2) * P))) {
+        (rc = alloc((void **)&Wd, sizeof(double) * 3 * 128 * 128)) || (rc = alloc((void **)&pairs_d, sizeof(int2) * P)) ||
+        (rc = alloc((void **)&errd, sizeof(int)))) {
         release();
         return rc;
     }
@@ -317,13 +403,13 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
     std::vector<int2> pairs(P);
     for (int j = 0; j < M; j++)
         for (int i = 0; i <= j; i++) pairs[pair_index(i, j)] = make_int2(i, j);
-#define RCK(x)                    \
-    do {                          \
-        cudaError_t e_ = (x);     \
-        if (e_ != cudaSuccess) {  \
-            release();            \
-            CUDA_OK(e_);          \
-        }                         \
+#define RCK(x)                        \
+    do {                              \
+        cudaError_t rck_ = (x);       \
+        if (rck_ != cudaSuccess) {    \
+            release();                \
+            CUDA_OK(rck_);            \
+        }                             \
     } while (0)
     RCK(cudaMemcpyAsync(wd, w.data(), sizeof(double) * SC, cudaMemcpyHostToDevice, st));
     RCK(cudaMemcpyAsync(V4, v4.data(), zsz * SC * 4, cudaMemcpyHostToDevice, st));
@@ -340,8 +426,31 @@ extern "C" int qd_coulomb_dev(const QdCoulombSpec *sp, const void *Zv, int64_t l
         return rc;
     }
     qd_count_launch(1);
-    coulomb_pair_kernel<<<dim3(blocks_for(S), P), 256, 0, st>>>(Fa, Fc, S, pairs_d, Bp);
-    RCK(cudaGetLastError());
+    if (M <= 32) {
+        // tiles of 16 points up to 16 states, 8 points up to 32 (at most 64 KB of shared memory, three
+        // blocks per SM); the 256 threads are tm points x 256 / tm pair groups
+        const int tm = M <= 16 ? 16 : 8;
+        const size_t smem = (size_t)2 * M * QD_N_BAND * tm * sizeof(double2);
+        static bool configured = false;
+        if (!configured) {
+            RCK(cudaFuncSetAttribute(coulomb_pair_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 140 * 1024));
+            configured = true;
+        }
+        RCK(cudaMemsetAsync(errd, 0, sizeof(int), st));
+        coulomb_pair_tma_kernel<<<(unsigned)((S + tm - 1) / tm), 256, smem, st>>>(Fa, Fc, S, M, tm, pairs_d, P, Bp,
+                                                                                   errd);
+        RCK(cudaGetLastError());
+        int herr = 0;
+        RCK(cudaMemcpyAsync(&herr, errd, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RCK(cudaStreamSynchronize(st));
+        if (herr) {
+            release();
+            return qd_set_error(QD_ERR_TIMEOUT, "qd_coulomb: staged pair products: wait for the bulk copies ran out");
+        }
+    } else {
+        coulomb_pair_kernel<<<dim3(blocks_for(S), P), 256, 0, st>>>(Fa, Fc, S, pairs_d, Bp);
+        RCK(cudaGetLastError());
+    }
     if ((rc = qd_dft3_batched(Bp, S, P, sz3, +1, st))) {
         release();
         return rc;
