@@ -22,6 +22,7 @@ typedef struct {
     qd_complex128 *const *eigvec;
     int *order;
     int next;
+    int sm_share; /* SMs each worker's solves spread over (0: the whole GPU) */
     int rc;
     char msg[512];
     pthread_mutex_t mu;
@@ -30,6 +31,7 @@ typedef struct {
 static void *batch_worker(void *arg) {
     batch_queue *q = (batch_queue *)arg;
     cudaSetDevice(q->device);
+    qd_set_sm_budget(q->sm_share);
     for (;;) {
         pthread_mutex_lock(&q->mu);
         int k = (q->rc == QD_OK && q->next < q->n) ? q->order[q->next++] : -1;
@@ -45,6 +47,7 @@ static void *batch_worker(void *arg) {
             pthread_mutex_unlock(&q->mu);
         }
     }
+    qd_set_sm_budget(0);
     return NULL;
 }
 
@@ -76,6 +79,16 @@ int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, d
     for (int i = 0; i < n; i++) q.order[i] = i;
     qsort_r(q.order, (size_t)n, sizeof(int), by_size_desc, problems);
     cudaGetDevice(&q.device);
+    /* Each worker's kernels spread over a share of the SMs (twice the even
+     * split, at least 16), so that the latency-bound stages of several
+     * instances run side by side instead of queueing behind kernels that take
+     * the whole GPU.  QD_BATCH_SMS overrides it (0: the whole GPU). */
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, q.device);
+    q.sm_share = n_threads > 1 ? 2 * nsm / n_threads : 0;
+    if (q.sm_share && q.sm_share < 16) q.sm_share = 16;
+    const char *env = getenv("QD_BATCH_SMS");
+    if (env) q.sm_share = atoi(env) > 0 ? atoi(env) : 0;
     pthread_mutex_init(&q.mu, NULL);
     /* handles of the threads that did start are kept contiguous, so only those are joined */
     int started = 0;

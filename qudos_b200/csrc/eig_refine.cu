@@ -309,7 +309,7 @@ extern "C" int qd_gram_ex_dev(int64_t n, const void *A, int64_t lda, int ka, con
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int64_t slices = 2 * (int64_t)nsm;
+    int64_t slices = 2 * (int64_t)qd_sm_budget(nsm);
     int64_t rows = (n + slices - 1) / slices;
     rows = ((rows + GR_ROWS - 1) / GR_ROWS) * GR_ROWS;
     const unsigned grid = (unsigned)((n + rows - 1) / rows);

@@ -445,7 +445,7 @@ static int launch_panel(T *P, int64_t lda, int m, int nb, int nref, T *Rp, T *ta
         CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     }
     int G = (m + 63) / 64;
-    if (G > nsm) G = nsm;
+    if (G > qd_sm_budget(nsm)) G = qd_sm_budget(nsm);
     if (G < 1) G = 1;
     int chunk = (m + G - 1) / G;
     size_t smem = (size_t)chunk * nb * sizeof(cpx<R>);

@@ -597,7 +597,7 @@ extern "C" int qd_hb2st(double2 *AB, int ldb, int n, int b, int *progress, int *
     const size_t smem = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hb2st_kernel, 256, smem));
     if (per_sm < 1) return qd_set_error(QD_ERR_CUDA, "hb2st kernel does not fit on an SM");
-    int G = nsm * per_sm;
+    int G = qd_sm_budget(nsm) * per_sm;
     int useful = n / (2 * b) + 2;  // concurrent sweeps are limited by the 2-task lag
     if (G > useful) G = useful;
     if (G > n - 1) G = n - 1;

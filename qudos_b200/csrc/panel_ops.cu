@@ -263,7 +263,7 @@ int nsm() {
         cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
         if (g_nsm < 1) g_nsm = 148;
     }
-    return g_nsm;
+    return qd_sm_budget(g_nsm);
 }
 
 // Rows per slice and slice count of tsmm_cn for m rows and k1 outputs per

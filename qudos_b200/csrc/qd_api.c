@@ -318,13 +318,13 @@ void qd_problem_free(qd_problem *pr) {
     for (int a = 0; a < 3; a++) {
         free(pr->G[a]);
         free(pr->GS[a]);
-        if (pr->d_G[a]) cudaFree(pr->d_G[a]);
-        if (pr->d_GS[a]) cudaFree(pr->d_GS[a]);
+        if (pr->d_G[a]) qd_pool_free(pr->d_G[a], NULL);
+        if (pr->d_GS[a]) qd_pool_free(pr->d_GS[a], NULL);
     }
     void *dev[] = {pr->d_geo, pr->d_mat, pr->d_chi_s, pr->d_eps_s, pr->d_phi_s, pr->d_chi,
                    pr->d_eps, pr->d_phi, pr->d_conv, pr->d_coef};
     for (size_t i = 0; i < sizeof(dev) / sizeof(dev[0]); i++)
-        if (dev[i]) cudaFree(dev[i]);
+        if (dev[i]) qd_pool_free(dev[i], NULL);
     free(pr->geo);
     free(pr->mat);
     free(pr);
@@ -505,8 +505,8 @@ static int assemble_from_globals(int n_shape, struct vector F, struct wave_vecto
                      : qd_assemble_dk_launch(d_coef, d_G, d_G + NT[0], d_G + NT[0] + NT[1], N, K, dk_axis, H_dev, ld,
                                              0, NULL);
     if (rc == QD_OK && cudaDeviceSynchronize() != cudaSuccess) rc = qd_set_error(QD_ERR_CUDA, "assembly failed");
-    cudaFree(d_coef);
-    cudaFree(d_G);
+    qd_pool_free(d_coef, NULL);
+    qd_pool_free(d_G, NULL);
     return rc;
 }
 
@@ -605,15 +605,15 @@ int qd_grad_contract(const void *d_dcoef, const double *d_Gx, const double *d_Gy
 /* Every device table of the problem is freed (the next build allocates anew). */
 static void release_tables(qd_problem *pr) {
     for (int a = 0; a < 3; a++) {
-        if (pr->d_G[a]) cudaFree(pr->d_G[a]);
-        if (pr->d_GS[a]) cudaFree(pr->d_GS[a]);
+        if (pr->d_G[a]) qd_pool_free(pr->d_G[a], NULL);
+        if (pr->d_GS[a]) qd_pool_free(pr->d_GS[a], NULL);
         pr->d_G[a] = NULL;
         pr->d_GS[a] = NULL;
     }
     void **dev[] = {&pr->d_geo, &pr->d_mat, &pr->d_chi_s, &pr->d_eps_s, &pr->d_phi_s, &pr->d_chi,
                     &pr->d_eps, &pr->d_phi, &pr->d_conv, &pr->d_coef};
     for (size_t i = 0; i < sizeof(dev) / sizeof(dev[0]); i++) {
-        if (*dev[i]) cudaFree(*dev[i]);
+        if (*dev[i]) qd_pool_free(*dev[i], NULL);
         *dev[i] = NULL;
     }
     pr->tables_ready = 0;
@@ -674,6 +674,10 @@ static void grad_units(int kind, double *floor_, double *to_user) {
         default: *floor_ = 1.0; *to_user = 1.0; break;                     /* relative scales */
     }
 }
+
+static __thread int g_sm_budget = 0;
+int qd_sm_budget(int nsm) { return g_sm_budget > 0 && g_sm_budget < nsm ? g_sm_budget : nsm; }
+void qd_set_sm_budget(int n) { g_sm_budget = n > 0 ? n : 0; }
 
 /* Contraction used by eigen_gradients_8_band: 0 = reciprocal-space
  * correlations by FFT (default), 1 = the direct sum over the lower triangle of

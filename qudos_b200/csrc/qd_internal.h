@@ -55,6 +55,11 @@ void qd_basis_grid(int n_T, double L, double *out);
 extern double qd_scale_Ep, qd_scale_gL1;
 
 void qd_count_launch(int n);
+/* SMs the calling host thread's solves may spread over: the device's count
+ * nsm, or the thread's budget when one is set (qd_set_sm_budget; the batched
+ * entry point gives each worker a share so that instances overlap). */
+int qd_sm_budget(int nsm);
+void qd_set_sm_budget(int n);
 
 /* Stream-ordered device allocations of the solve path, served from the
  * device's default memory pool with its release threshold raised, so that

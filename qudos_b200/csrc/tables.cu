@@ -1058,8 +1058,9 @@ static int upload_gl_rule() {
 
 template <class T>
 static int dalloc(T **p, size_t bytes) {
-    cudaError_t e = cudaMalloc((void **)p, bytes ? bytes : 16);
-    if (e != cudaSuccess) return qd_set_error(QD_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    // stream-ordered pool (per-thread default stream): unlike cudaMalloc / cudaFree it does not
+    // synchronise the device, so table builds of concurrent solves do not stall each other
+    if (qd_pool_alloc((void **)p, bytes, 0) != 0) return qd_set_error(QD_ERR_NOMEM, "device allocation of %zu bytes", bytes);
     return QD_OK;
 }
 
@@ -1187,9 +1188,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             }
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(st));
-            cudaFree(corr);
-            cudaFree(conv);
-            cudaFree(work);
+            qd_pool_free(corr, 0);
+            qd_pool_free(conv, 0);
+            qd_pool_free(work, 0);
         }
         if (P.piezo != 0) {
             Grid3 pg = {{smooth_size(2 * pr->NTS[0] - 1), smooth_size(2 * pr->NTS[1] - 1),
@@ -1246,9 +1247,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             }
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(st));
-            cudaFree(work);
-            cudaFree(ctab);
-            if (prod) cudaFree(prod);
+            qd_pool_free(work, 0);
+            qd_pool_free(ctab, 0);
+            if (prod) qd_pool_free(prod, 0);
         }
         // electronic-cell chi: copy when the cells coincide (8_band_main.c:425-442)
         if (pr->same_cells) {
@@ -1294,9 +1295,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
             }
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(st));
-            cudaFree(W);
-            cudaFree(t0);
-            cudaFree(t1);
+            qd_pool_free(W, 0);
+            qd_pool_free(t0, 0);
+            qd_pool_free(t1, 0);
         } else {
             int same[3];
             for (int a = 0; a < 3; a++) {
@@ -1336,7 +1337,7 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
         }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
-        cudaFree(work);
+        qd_pool_free(work, 0);
     } else if (ns > 1) {
         chi_kernel<<<dim3(nblk(nT, 128), ns - 1), 128, 0, st>>>(dg, 1, ns, pr->d_G[0], pr->d_G[1], pr->d_G[2],
                                                                  pr->NT[0], pr->NT[1], pr->NT[2], 0, P.softening,
@@ -1381,9 +1382,9 @@ extern "C" int qd_tables_tangent_dev(struct qd_problem *pr, const struct materia
             (const double2 *)pr->d_chi, (const double2 *)pr->d_eps, nullptr, (const double2 *)pr->d_conv,
             (double2 *)dcoef);
         e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     }
-    cudaFree(dm);
+    qd_pool_free(dm, 0);
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "tangent table: %s", cudaGetErrorString(e));
     return QD_OK;
 }
@@ -1438,10 +1439,10 @@ extern "C" int qd_coef_from_host_tables(int n_shape, const int N[3], const doubl
     CK(cudaMemcpy(dG, Gx, sizeof(double) * NT[0], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dG + NT[0], Gy, sizeof(double) * NT[1], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dG + NT[0] + NT[1], Gz, sizeof(double) * NT[2], cudaMemcpyHostToDevice));
-    cudaFree(dg); cudaFree(dm); cudaFree(chi);
-    if (eps) cudaFree(eps);
-    if (phi) cudaFree(phi);
-    if (conv) cudaFree(conv);
+    qd_pool_free(dg, 0); qd_pool_free(dm, 0); qd_pool_free(chi, 0);
+    if (eps) qd_pool_free(eps, 0);
+    if (phi) qd_pool_free(phi, 0);
+    if (conv) qd_pool_free(conv, 0);
     *d_coef_out = coef;
     *d_G_out = dG;
     return QD_OK;

@@ -929,7 +929,7 @@ int sm_count() {
         cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
         if (g_nsm <= 0) g_nsm = 148;
     }
-    return g_nsm;
+    return qd_sm_budget(g_nsm);
 }
 
 constexpr int SMEM_EXTRA = 1024 /*alignment*/ + 512 /*barriers*/;
