@@ -353,9 +353,14 @@ int qd_tuning_set(int prec, int64_t n_h_max, int agg);
  * H is linear in the per-difference coefficient tables, so dH/dp is the
  * Hamiltonian of dcoef/dp.  For the field and the Ep and gamma_1 scales that
  * table derivative is exact (the table is linear in the field and in the
- * material parameters, whose derivatives are closed forms); for lengths and
- * composition it is a central difference of two table builds (step rel_step
- * times the parameter's magnitude, with a floor; rel_step <= 0 selects 1e-4).
+ * material parameters, whose derivatives are closed forms).  A length moves
+ * only its shape's transform chi: dchi/dL is a fourth-order central
+ * difference of the closed-form transform, and the table, a polynomial in
+ * chi, is differentiated along it exactly by builds at chi +- dir (and
+ * +- 2 dir when second-order piezo or position-dependent elastic constants
+ * raise its degree).  Composition: a central difference of two table builds.
+ * Steps: rel_step times the parameter's magnitude, with a floor (rel_step <= 0
+ * selects 1e-4).
  * The contraction never forms dH: every band function is a bilinear form in
  * G + K and G' + K, so <psi|dH|psi> = Re sum_f sum_D dcoef_f(D) C_f(D) with
  * C_f the reciprocal-space correlations of the k-weighted envelopes, computed

@@ -502,6 +502,24 @@ __global__ void coef_diff_kernel(const double2 *plus, const double2 *minus, int6
 }
 }  // namespace
 
+// d = scale (8 (p1 - m1) - (p2 - m2)): the four-point central difference
+__global__ void coef_diff4_kernel(const double2 *p1, const double2 *m1, const double2 *p2, const double2 *m2, int64_t n,
+                                  double scale, double2 *d) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        d[t] = make_double2(scale * (8.0 * (p1[t].x - m1[t].x) - (p2[t].x - m2[t].x)),
+                            scale * (8.0 * (p1[t].y - m1[t].y) - (p2[t].y - m2[t].y)));
+}
+extern "C" int qd_coef_diff4(const void *p1, const void *m1, const void *p2, const void *m2, int64_t n, double scale,
+                             void *d, void *stream) {
+    qd_count_launch(1);
+    coef_diff4_kernel<<<1024, 256, 0, (cudaStream_t)stream>>>((const double2 *)p1, (const double2 *)m1,
+                                                              (const double2 *)p2, (const double2 *)m2, n, scale,
+                                                              (double2 *)d);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "coef diff4: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
 extern "C" int qd_coef_diff(const void *plus, const void *minus, int64_t n, double scale, void *d, void *stream) {
     qd_count_launch(1);
     coef_diff_kernel<<<1024, 256, 0, (cudaStream_t)stream>>>((const double2 *)plus, (const double2 *)minus, n, scale,

@@ -599,6 +599,9 @@ void coulomb_matrix_elements(struct wave_vectors basis, struct wave_vectors coul
 /* Hellmann-Feynman gradients of the window's eigenvalues                     */
 /* ------------------------------------------------------------------------- */
 int qd_coef_diff(const void *plus, const void *minus, int64_t n, double scale, void *d, void *stream);
+int qd_coef_diff4(const void *p1, const void *m1, const void *p2, const void *m2, int64_t n, double scale, void *d,
+                  void *stream);
+int qd_chi_direction(struct qd_problem *pr, int s, const struct supercell_geometry *geo4, void **dir_s, void **dir);
 int qd_grad_contract(const void *d_dcoef, const double *d_Gx, const double *d_Gy, const double *d_Gz, const int N[3],
                      const double K[3], const void *psi, int64_t ldz, int m, double *out_dev, void *stream);
 
@@ -700,7 +703,7 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
     if (!(rel_step > 0.0)) rel_step = 1e-4;
     RC(qd_problem_build_tables(pr));
     const int64_t nt = pr->nT, ncoef = (int64_t)QD_N_COEF * nt, nh = pr->n_h;
-    void *Z = NULL, *dplus = NULL, *dminus = NULL, *dcoef = NULL;
+    void *Z = NULL, *dplus = NULL, *dminus = NULL, *dcoef = NULL, *dplus2 = NULL, *dminus2 = NULL;
     double *out = NULL;
     int rc = QD_OK;
     if (qd_pool_alloc(&Z, sizeof(qd_complex128) * (size_t)nh * n_states, NULL) ||
@@ -749,6 +752,60 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
                     break;
                 }
                 if ((rc = qd_tables_tangent_dev(pr, dmat, dF, dcoef))) break;
+            } else if (q->kind == QD_GRAD_LENGTH || q->kind == QD_GRAD_BASE) {
+                /* A length moves only chi of its shape.  dchi/dL: fourth-order central difference
+                 * of the closed-form transforms (steps +-h, +-2h).  The table is a polynomial in chi
+                 * (strain linear, convolutions and first-order piezo quadratic, second-order piezo
+                 * and the position-dependent elastic series of higher degree), so its derivative
+                 * along dir = h dchi/dL is taken exactly by builds at chi + t dir: t = +-1 (exact to
+                 * degree 2), or +-1, +-2 (exact to degree 4) when second-order piezo or
+                 * position-dependent elastic constants raise the degree. */
+                double v0 = 0.0, floor_ = 1.0, to_user = 1.0, dummy;
+                if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
+                grad_units(q->kind, &floor_, &to_user);
+                const double h = rel_step * (fabs(v0) > floor_ ? fabs(v0) : floor_);
+                struct supercell_geometry *g4 = (struct supercell_geometry *)malloc(sizeof(*g4) * 4 * (size_t)ns);
+                if (!g4) {
+                    rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band");
+                    break;
+                }
+                const double del[4] = {2.0 * h, h, -h, -2.0 * h};
+                for (int k4 = 0; rc == QD_OK && k4 < 4; k4++) {
+                    rc = grad_apply(pr, q, del[k4], &dummy);
+                    memcpy(g4 + (size_t)k4 * ns, pr->geo, sizeof(*g4) * ns);
+                    memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
+                    pr->p = p0;
+                    if (rc == QD_OK) rc = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+                }
+                void *dir_s = NULL, *dir = NULL;
+                if (rc == QD_OK) rc = qd_chi_direction(pr, q->shape, g4, &dir_s, &dir);
+                free(g4);
+                const int four = pr->p.piezo >= 2 || pr->p.elastic_const != 0;
+                if (rc == QD_OK && four && !dplus2 &&
+                    (qd_pool_alloc(&dplus2, sizeof(qd_complex128) * (size_t)ncoef, NULL) ||
+                     qd_pool_alloc(&dminus2, sizeof(qd_complex128) * (size_t)ncoef, NULL)))
+                    rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band: work buffers");
+                const double ts[4] = {1.0, -1.0, 2.0, -2.0};
+                void *outs[4] = {dplus, dminus, dplus2, dminus2};
+                pr->chi_dir_shape = q->shape;
+                pr->d_chi_dir_s = dir_s;
+                pr->d_chi_dir = dir;
+                for (int k4 = 0; rc == QD_OK && k4 < (four ? 4 : 2); k4++) {
+                    pr->chi_dir_t = ts[k4];
+                    release_tables(pr);
+                    if ((rc = qd_tables_build_dev(pr))) break;
+                    if (cudaMemcpy(outs[k4], pr->d_coef, sizeof(qd_complex128) * (size_t)ncoef,
+                                   cudaMemcpyDeviceToDevice) != cudaSuccess)
+                        rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: table copy");
+                }
+                pr->chi_dir_t = 0.0;
+                pr->d_chi_dir_s = pr->d_chi_dir = NULL;
+                qd_pool_free(dir_s, NULL);
+                qd_pool_free(dir, NULL);
+                if (rc) break;
+                rc = four ? qd_coef_diff4(dplus, dminus, dplus2, dminus2, ncoef, 1.0 / (12.0 * h), dcoef, NULL)
+                          : qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL);
+                if (rc) break;
             } else {
                 double v0 = 0.0, floor_ = 1.0, to_user = 1.0;
                 if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
@@ -800,7 +857,7 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
             for (int s = 0; s < n_states; s++) dEdp[(size_t)k * n_states + s] *= to_user;
         }
     }
-    void *bufs[] = {Z, dplus, dminus, dcoef, out, corr};
+    void *bufs[] = {Z, dplus, dminus, dcoef, out, corr, dplus2, dminus2};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i]) qd_pool_free(bufs[i], NULL);
     return rc;

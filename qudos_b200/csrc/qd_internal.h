@@ -43,6 +43,12 @@ struct qd_problem {
     void *d_chi, *d_eps, *d_phi, *d_conv; /* electronic cell: chi [n_shape][nT], eps[6], phi, conv [n_shape][8] */
     void *d_coef;                        /* fused coefficients [QD_N_COEF][nT] */
     int tables_ready;
+    /* table builds for a directional derivative: chi of shape chi_dir_shape is
+     * shifted by chi_dir_t times the direction arrays (strain cell [nTS],
+     * electronic cell [nT]; device) when chi_dir_t != 0 */
+    int chi_dir_shape;
+    double chi_dir_t;
+    void *d_chi_dir_s, *d_chi_dir;
 };
 
 /* host_inputs.c */

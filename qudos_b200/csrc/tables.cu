@@ -467,6 +467,29 @@ __global__ void chi_kernel(const geo_t *geo, int s0, int s1, const double *Gx, c
     out[(int64_t)s * n + t] = chi_point(Gx[ix], Gy[iy], Gz[iz], geo, s, cell, softening, sigma).d2();
 }
 
+// y += t x over n complex values
+__global__ void axpy_kernel(double2 *y, const double2 *x, double t, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = make_double2(y[i].x + t * x[i].x, y[i].y + t * x[i].y);
+}
+
+// Fourth-order central difference of shape s's transform along a geometry
+// parameter: geo4 holds four copies of the shapes with that parameter at
+// +2h, +h, -h, -2h; out = (-chi(+2h) + 8 chi(+h) - 8 chi(-h) + chi(-2h)) / 12,
+// which is h dchi/dp to O(h^5).
+__global__ void chi_direction_kernel(const geo_t *geo4, int ns, int s, const double *Gx, const double *Gy,
+                                     const double *Gz, int nx, int ny, int nz, int cell, int softening, double sigma,
+                                     double2 *out) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int ix = (int)(t / ((int64_t)ny * nz)), iy = (int)((t / nz) % ny), iz = (int)(t % nz);
+    const double w[4] = {-1.0 / 12.0, 8.0 / 12.0, -8.0 / 12.0, 1.0 / 12.0};
+    zc acc(0.0);
+    for (int k = 0; k < 4; k++) acc += w[k] * chi_point(Gx[ix], Gy[iy], Gz[iz], geo4 + k * ns, s, cell, softening, sigma);
+    out[t] = acc.d2();
+}
+
 // --------------------------------------------------------------------------
 // Strain (strain_fourier_coefficient.c:108-173), position-independent elastic constants
 // --------------------------------------------------------------------------
@@ -1143,6 +1166,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
                                                                       pr->NTS[0], pr->NTS[1], pr->NTS[2], 1,
                                                                       P.softening, P.sigma, chi_s);
             CK(cudaGetLastError());
+            if (pr->chi_dir_t != 0.0 && pr->d_chi_dir_s)
+                axpy_kernel<<<nblk(nTS, 256), 256, 0, st>>>(chi_s + (int64_t)pr->chi_dir_shape * nTS,
+                                                            (const double2 *)pr->d_chi_dir_s, pr->chi_dir_t, nTS);
         }
         // isotropic approximation (strain_region_reciprocal_space.c:28-40) mutates C44 of every shape
         if (P.isotropic != 0) {
@@ -1259,6 +1285,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
                                                                      pr->NT[0], pr->NT[1], pr->NT[2], 0, P.softening,
                                                                      P.sigma, chi);
             CK(cudaGetLastError());
+            if (pr->chi_dir_t != 0.0 && pr->d_chi_dir)
+                axpy_kernel<<<nblk(nT, 256), 256, 0, st>>>(chi + (int64_t)pr->chi_dir_shape * nT,
+                                                           (const double2 *)pr->d_chi_dir, pr->chi_dir_t, nT);
         }
         // downsample strain and phi (free lengths, identity when the cells coincide; or commensurate lengths)
         RC(dalloc(&eps, sizeof(double2) * nT * 6));
@@ -1343,6 +1372,9 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
                                                                  pr->NT[0], pr->NT[1], pr->NT[2], 0, P.softening,
                                                                  P.sigma, chi);
         CK(cudaGetLastError());
+        if (pr->chi_dir_t != 0.0 && pr->d_chi_dir)
+            axpy_kernel<<<nblk(nT, 256), 256, 0, st>>>(chi + (int64_t)pr->chi_dir_shape * nT,
+                                                       (const double2 *)pr->d_chi_dir, pr->chi_dir_t, nT);
     }
     // fused per-difference coefficients
     double2 *coef;
@@ -1386,6 +1418,38 @@ extern "C" int qd_tables_tangent_dev(struct qd_problem *pr, const struct materia
     }
     qd_pool_free(dm, 0);
     if (e != cudaSuccess) return qd_set_error(QD_ERR_CUDA, "tangent table: %s", cudaGetErrorString(e));
+    return QD_OK;
+}
+
+// Direction arrays for a derivative along one geometry parameter of shape s:
+// geo4 holds four host copies of the problem's shapes with that parameter at
+// +2h, +h, -h, -2h.  Allocates *dir_s (strain cell, when strain is on) and
+// *dir (electronic cell) = h dchi_s/dp to O(h^5); free with qd_pool_free.
+extern "C" int qd_chi_direction(struct qd_problem *pr, int s, const struct supercell_geometry *geo4, void **dir_s,
+                                void **dir) {
+    if (!pr->tables_ready) return qd_set_error(QD_ERR_ARG, "qd_chi_direction: tables not built");
+    const qd_params &P = pr->p;
+    const int ns = P.n_shape;
+    if (s < 1 || s >= ns) return qd_set_error(QD_ERR_ARG, "qd_chi_direction: shape %d", s);
+    cudaStream_t st = 0;
+    geo_t *dg4 = nullptr;
+    double2 *ds = nullptr, *de = nullptr;
+    RC(dalloc(&dg4, sizeof(geo_t) * 4 * ns));
+    CK(cudaMemcpy(dg4, geo4, sizeof(geo_t) * 4 * ns, cudaMemcpyHostToDevice));
+    if (P.strain) {
+        RC(dalloc(&ds, sizeof(double2) * pr->nTS));
+        chi_direction_kernel<<<nblk(pr->nTS, 128), 128, 0, st>>>(dg4, ns, s, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
+                                                                 pr->NTS[0], pr->NTS[1], pr->NTS[2], 1, P.softening,
+                                                                 P.sigma, ds);
+    }
+    RC(dalloc(&de, sizeof(double2) * pr->nT));
+    chi_direction_kernel<<<nblk(pr->nT, 128), 128, 0, st>>>(dg4, ns, s, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0],
+                                                            pr->NT[1], pr->NT[2], 0, P.softening, P.sigma, de);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    qd_pool_free(dg4, 0);
+    *dir_s = ds;
+    *dir = de;
     return QD_OK;
 }
 

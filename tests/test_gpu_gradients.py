@@ -121,3 +121,23 @@ def test_fft_correlation_matches_direct_contraction(base_solution):
         method.value = 0
     scale = np.abs(gd).max(axis=1, keepdims=True)
     assert np.all(np.abs(g - gd) <= 1e-10 * scale), np.abs(g - gd).max(axis=1) / scale[:, 0]
+
+
+@pytest.mark.parametrize("name", ["height", "half_base"])
+def test_length_gradients_with_second_order_piezo(tmp_path, name):
+    """Second-order piezoelectricity makes the coefficient table a polynomial
+    of degree above two in the shape functions; the length derivatives then
+    take the four-point stencil along dchi/dL.  Against central differences
+    of full FP64 solves (relative step 1e-5), 7^3 plane waves."""
+    ov = ("-Piezo=2",)
+    d = _deck(tmp_path, "base", 3)
+    pr = q.Problem(d, ov)
+    w, v = pr.solve(q.QD_PREC_FP64)
+    k = [p for p, _ in PARAMS].index(name)
+    g = pr.gradients(v, [PARAMS[k][1]])[0]
+    h = 1e-5 * max(abs(BASE[name]), 1.0)
+    wp = q.Problem(_deck(tmp_path, "p", 3, **{name: BASE[name] + h}), ov).solve(q.QD_PREC_FP64)[0]
+    wm = q.Problem(_deck(tmp_path, "m", 3, **{name: BASE[name] - h}), ov).solve(q.QD_PREC_FP64)[0]
+    fd = _pairs((wp - wm) / (2 * h))
+    ad = _pairs(g)
+    assert np.abs(ad - fd).max() <= 1e-4 * np.abs(fd).max(), (name, ad, fd)
