@@ -99,3 +99,22 @@ def test_coulomb_golden_direct_terms(example):
     ours = coulomb.direct_pair_terms(out, nv, nc)
     for k in ("hh", "ee", "eh"):
         assert np.abs(ours[k] - np.array(gold[k])).max() < 2e-10, k
+
+
+def test_staged_and_plain_pair_products_agree(tmp_path):
+    """Up to 32 states the pair products stage their operands by TMA bulk
+    copies (8-point tiles above 16 states); above 32 the plain kernel runs.
+    The conduction-conduction elements depend on the conduction states only,
+    so 16 valence + 16 conduction states (staged) and 18 + 16 (plain) with the
+    same conduction vectors must give the same ee elements."""
+    d = _deck(tmp_path, 2, 2, 1)
+    prob = q.Problem(d)
+    rng = np.random.default_rng(11)
+    n_h = prob.n_h
+    v = rng.normal(size=(n_h, 34)) + 1j * rng.normal(size=(n_h, 34))
+    v /= np.linalg.norm(v, axis=0)
+    plain = prob.coulomb(v, 18, 16, madelung_ranks=1)
+    staged = prob.coulomb(np.concatenate([v[:, 2:18], v[:, 18:]], axis=1), 16, 16, madelung_ranks=1)
+    scale = np.abs(plain["ee"]).max()
+    assert scale > 0
+    assert np.abs(staged["ee"] - plain["ee"]).max() <= 1e-12 * scale
