@@ -358,7 +358,10 @@ int qd_tuning_set(int prec, int64_t n_h_max, int agg);
  * difference of the closed-form transform, and the table, a polynomial in
  * chi, is differentiated along it exactly by builds at chi +- dir (and
  * +- 2 dir when second-order piezo or position-dependent elastic constants
- * raise its degree).  Composition: a central difference of two table builds.
+ * raise its degree).  Composition moves only the shape's material
+ * parameters, in which the table is a polynomial too: dmat/dx is a
+ * fourth-order central difference of the host material function and the
+ * table is differentiated along it the same way.
  * Steps: rel_step times the parameter's magnitude, with a floor (rel_step <= 0
  * selects 1e-4).
  * The contraction never forms dH: every band function is a bilinear form in

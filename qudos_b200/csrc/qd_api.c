@@ -806,6 +806,61 @@ int eigen_gradients_8_band(qd_problem *pr, const qd_complex128 *eigvec_host, int
                 rc = four ? qd_coef_diff4(dplus, dminus, dplus2, dminus2, ncoef, 1.0 / (12.0 * h), dcoef, NULL)
                           : qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL);
                 if (rc) break;
+            } else if (q->kind == QD_GRAD_COMPOSITION) {
+                /* The composition moves only the composed shape's material parameters, and for a
+                 * fixed geometry the table is a polynomial in them (the mismatch (a_emb - a_s) /
+                 * a_matrix is linear in a_s; band parameters, P and deformation potentials enter
+                 * linearly, products with the strain give degree two, second-order piezo and the
+                 * position-dependent elastic series more).  dmat/dx: fourth-order central
+                 * difference of the host material function (steps +-h, +-2h); the table's
+                 * derivative along dmat is then exact from builds at mat +- t dmat. */
+                double v0 = 0.0, floor_ = 1.0, to_user = 1.0, dummy;
+                if ((rc = grad_apply(pr, q, 0.0, &v0))) break;
+                grad_units(q->kind, &floor_, &to_user);
+                const double h = rel_step * (fabs(v0) > floor_ ? fabs(v0) : floor_);
+                const size_t nd = sizeof(struct material_params) / sizeof(double);
+                double *m4 = (double *)malloc(sizeof(struct material_params) * 5 * (size_t)ns);
+                if (!m4) {
+                    rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band");
+                    break;
+                }
+                double *mat0 = m4 + 4 * nd * (size_t)ns;
+                const double del[4] = {2.0 * h, h, -h, -2.0 * h};
+                for (int k4 = 0; rc == QD_OK && k4 < 4; k4++) {
+                    rc = grad_apply(pr, q, del[k4], &dummy);
+                    memcpy(m4 + (size_t)k4 * nd * ns, pr->mat, sizeof(struct material_params) * ns);
+                    memcpy(pr->geo, geo0, sizeof(*geo0) * ns);
+                    pr->p = p0;
+                    if (rc == QD_OK) rc = qd_material_parameters(pr->p.T, pr->p.piezo, ns, pr->geo, pr->mat);
+                }
+                if (rc == QD_OK) memcpy(mat0, pr->mat, sizeof(struct material_params) * ns);
+                const int four = pr->p.piezo >= 2 || pr->p.elastic_const != 0;
+                if (rc == QD_OK && four && !dplus2 &&
+                    (qd_pool_alloc(&dplus2, sizeof(qd_complex128) * (size_t)ncoef, NULL) ||
+                     qd_pool_alloc(&dminus2, sizeof(qd_complex128) * (size_t)ncoef, NULL)))
+                    rc = qd_set_error(QD_ERR_NOMEM, "eigen_gradients_8_band: work buffers");
+                const double ts[4] = {1.0, -1.0, 2.0, -2.0};
+                void *outs[4] = {dplus, dminus, dplus2, dminus2};
+                for (int k4 = 0; rc == QD_OK && k4 < (four ? 4 : 2); k4++) {
+                    double *mp = (double *)pr->mat;
+                    for (size_t e = 0; e < nd * (size_t)ns; e++) {
+                        const size_t o = e;  /* field e % nd of shape e / nd */
+                        const double dm = (-m4[o] + 8.0 * m4[nd * ns + o] - 8.0 * m4[2 * nd * ns + o] +
+                                           m4[3 * nd * ns + o]) / 12.0;
+                        mp[e] = mat0[e] + ts[k4] * dm;
+                    }
+                    release_tables(pr);
+                    if ((rc = qd_tables_build_dev(pr))) break;
+                    if (cudaMemcpy(outs[k4], pr->d_coef, sizeof(qd_complex128) * (size_t)ncoef,
+                                   cudaMemcpyDeviceToDevice) != cudaSuccess)
+                        rc = qd_set_error(QD_ERR_CUDA, "eigen_gradients_8_band: table copy");
+                }
+                memcpy(pr->mat, mat0, sizeof(struct material_params) * ns);
+                free(m4);
+                if (rc) break;
+                rc = four ? qd_coef_diff4(dplus, dminus, dplus2, dminus2, ncoef, 1.0 / (12.0 * h), dcoef, NULL)
+                          : qd_coef_diff(dplus, dminus, ncoef, 1.0 / (2.0 * h), dcoef, NULL);
+                if (rc) break;
             } else {
                 double v0 = 0.0, floor_ = 1.0, to_user = 1.0;
                 if ((rc = grad_apply(pr, q, 0.0, &v0))) break;

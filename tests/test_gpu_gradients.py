@@ -123,12 +123,13 @@ def test_fft_correlation_matches_direct_contraction(base_solution):
     assert np.all(np.abs(g - gd) <= 1e-10 * scale), np.abs(g - gd).max(axis=1) / scale[:, 0]
 
 
-@pytest.mark.parametrize("name", ["height", "half_base"])
-def test_length_gradients_with_second_order_piezo(tmp_path, name):
+@pytest.mark.parametrize("name", ["height", "half_base", "x"])
+def test_gradients_with_second_order_piezo(tmp_path, name):
     """Second-order piezoelectricity makes the coefficient table a polynomial
-    of degree above two in the shape functions; the length derivatives then
-    take the four-point stencil along dchi/dL.  Against central differences
-    of full FP64 solves (relative step 1e-5), 7^3 plane waves."""
+    of degree above two in the shape functions and in the material
+    parameters; the length and composition derivatives then take the
+    four-point stencil along dchi/dL and dmat/dx.  Against central
+    differences of full FP64 solves (relative step 1e-5), 7^3 plane waves."""
     ov = ("-Piezo=2",)
     d = _deck(tmp_path, "base", 3)
     pr = q.Problem(d, ov)
