@@ -328,7 +328,9 @@ int qd_stage1_profile(double *ms, int n);
  * eigvec[k]) (host outputs of M_k and N_H,k x M_k values).  Up to n_threads
  * solves run at once, each from its own host thread on its own stream,
  * largest instances first, so that small latency-bound solves overlap on the
- * GPU.  Returns the first failure. */
+ * GPU.  Each worker's kernels size their grids to a share of the SMs (twice
+ * the even split, at least 16; the environment's QD_BATCH_SMS sets it, 0 for
+ * the whole GPU).  Returns the first failure. */
 int eigenstates_batched(qd_problem **problems, int n, int prec, int n_threads, double *const *eigval,
                         qd_complex128 *const *eigvec);
 
