@@ -3,10 +3,11 @@
 //
 //   1. padded envelopes a_sb and conjugate-reversed copies per state and band
 //      on the (2Nx-1)(2Ny-1)(2Nz-1) grid (state_redistribution.c:45-66);
-//   2. batched 3-D DFTs of all of them (per-axis direct DFTs; the sizes are
-//      odd and often prime);
+//   2. batched 3-D FFTs of all of them (the library's mixed-radix kernels; the
+//      (2N - 1) sizes are odd, prime factors above 7 are one DFT stage each);
 //   3. for every pair p = (i <= j) the band-summed pointwise product
-//      sum_b conj-rev(a_ib)^ . (a_jb)^, and ONE inverse DFT per pair (the
+//      sum_b conj-rev(a_ib)^ . (a_jb)^ (operands staged by TMA bulk copies up
+//      to 32 states), and ONE inverse FFT per pair (the
 //      reference transforms back per band and then adds; the transform is
 //      linear, so summing first is the same B_ij, B_convolutions.c:332-390);
 //   4. B on the Coulomb-cell grid: a scaled copy when the cells agree, else

@@ -10,9 +10,9 @@
 //   fused per-difference coefficients      (feeds the assembly kernel)
 //
 // Grids are (N_xT, N_yT, N_zT) with flat index iz + N_zT (iy + N_yT ix).  The
-// reference's zero-padded FFT convolutions on the (2 N_T - 1)^3 grid are done
-// with per-axis direct DFT kernels (every axis length here is odd and <= ~160,
-// so an O(n^2) line transform in shared memory is exact to rounding and cheap).
+// reference's zero-padded FFT convolutions are done on padded grids of at
+// least 2 N_T - 1 points per axis, rounded up to sizes with factors 2, 3, 5, 7,
+// with the batched mixed-radix FFT kernels below.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -681,8 +681,6 @@ __global__ void mul_kernel(const double2 *a, int64_t sa, const double2 *c, int64
     out[b * so + t] = (x * y).d2();
 }
 
-// In-place 1-D DFT along one axis for nb arrays: X[k] = sum_j x[j] exp(sign 2 pi i j k / n).
-// One block per line; line and twiddles in shared memory.
 // Batched 1-D FFTs along one axis of nb three-dimensional arrays: mixed-radix
 // Stockham (self-sorting) transforms in shared memory, LPB lines per block.
 // A stage of radix R over a line of n points with Ns = product of the radices
