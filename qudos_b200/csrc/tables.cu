@@ -476,18 +476,27 @@ __global__ void axpy_kernel(double2 *y, const double2 *x, double t, int64_t n) {
 // Fourth-order central difference of shape s's transform along a geometry
 // parameter: geo4 holds four copies of the shapes with that parameter at
 // +2h, +h, -h, -2h; out = (-chi(+2h) + 8 chi(+h) - 8 chi(-h) + chi(-2h)) / 12,
-// which is h dchi/dp to O(h^5).
-__global__ void chi_direction_kernel(const geo_t *geo4, int ns, int s, const double *Gx, const double *Gy,
-                                     const double *Gz, int nx, int ny, int nz, int cell, int softening, double sigma,
-                                     double2 *out) {
+// which is h dchi/dp to O(h^5).  Block (32, 4): threadIdx.y picks the stencil
+// point, so the four evaluations of one grid point run on four warps and a
+// small grid still spreads over every SM; the sum keeps the order k = 0..3.
+__global__ void __launch_bounds__(128) chi_direction_kernel(const geo_t *geo4, int ns, int s, const double *Gx,
+                                                            const double *Gy, const double *Gz, int nx, int ny, int nz,
+                                                            int cell, int softening, double sigma, double2 *out) {
+    __shared__ double2 part[4][32];
     const int64_t n = (int64_t)nx * ny * nz;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int ix = (int)(t / ((int64_t)ny * nz)), iy = (int)((t / nz) % ny), iz = (int)(t % nz);
+    const int64_t t = blockIdx.x * (int64_t)32 + threadIdx.x;
+    const int k = threadIdx.y;
     const double w[4] = {-1.0 / 12.0, 8.0 / 12.0, -8.0 / 12.0, 1.0 / 12.0};
-    zc acc(0.0);
-    for (int k = 0; k < 4; k++) acc += w[k] * chi_point(Gx[ix], Gy[iy], Gz[iz], geo4 + k * ns, s, cell, softening, sigma);
-    out[t] = acc.d2();
+    if (t < n) {
+        const int ix = (int)(t / ((int64_t)ny * nz)), iy = (int)((t / nz) % ny), iz = (int)(t % nz);
+        part[k][threadIdx.x] = (w[k] * chi_point(Gx[ix], Gy[iy], Gz[iz], geo4 + k * ns, s, cell, softening, sigma)).d2();
+    }
+    __syncthreads();
+    if (k == 0 && t < n) {
+        zc acc(0.0);
+        for (int j = 0; j < 4; j++) acc += zc(part[j][threadIdx.x].x, part[j][threadIdx.x].y);
+        out[t] = acc.d2();
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -1436,12 +1445,12 @@ extern "C" int qd_chi_direction(struct qd_problem *pr, int s, const struct super
     CK(cudaMemcpy(dg4, geo4, sizeof(geo_t) * 4 * ns, cudaMemcpyHostToDevice));
     if (P.strain) {
         RC(dalloc(&ds, sizeof(double2) * pr->nTS));
-        chi_direction_kernel<<<nblk(pr->nTS, 128), 128, 0, st>>>(dg4, ns, s, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
+        chi_direction_kernel<<<nblk(pr->nTS, 32), dim3(32, 4), 0, st>>>(dg4, ns, s, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
                                                                  pr->NTS[0], pr->NTS[1], pr->NTS[2], 1, P.softening,
                                                                  P.sigma, ds);
     }
     RC(dalloc(&de, sizeof(double2) * pr->nT));
-    chi_direction_kernel<<<nblk(pr->nT, 128), 128, 0, st>>>(dg4, ns, s, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0],
+    chi_direction_kernel<<<nblk(pr->nT, 32), dim3(32, 4), 0, st>>>(dg4, ns, s, pr->d_G[0], pr->d_G[1], pr->d_G[2], pr->NT[0],
                                                             pr->NT[1], pr->NT[2], 0, P.softening, P.sigma, de);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
