@@ -456,6 +456,9 @@ __device__ zc chi_point(double Gx0, double Gy0, double Gz0, const geo_t *geo, in
     return r;
 }
 
+// One thread per grid point (ix, iy, iz) and shape s0 + blockIdx.y.  Launched
+// with 64-thread blocks: the transforms are FP64-latency bound and a small
+// grid (21^3 points) then still spreads over every SM.
 __global__ void chi_kernel(const geo_t *geo, int s0, int s1, const double *Gx, const double *Gy,
                            const double *Gz, int nx, int ny, int nz, int cell, int softening, double sigma,
                            double2 *out) {
@@ -1169,7 +1172,7 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
         CK(cudaMemset(phi_s, 0, sizeof(double2) * nTS));
         pr->d_chi_s = chi_s; pr->d_eps_s = eps_s; pr->d_phi_s = phi_s;
         if (ns > 1) {
-            chi_kernel<<<dim3(nblk(nTS, 128), ns - 1), 128, 0, st>>>(dg, 1, ns, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
+            chi_kernel<<<dim3(nblk(nTS, 64), ns - 1), 64, 0, st>>>(dg, 1, ns, pr->d_GS[0], pr->d_GS[1], pr->d_GS[2],
                                                                       pr->NTS[0], pr->NTS[1], pr->NTS[2], 1,
                                                                       P.softening, P.sigma, chi_s);
             CK(cudaGetLastError());
@@ -1288,7 +1291,7 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
         if (pr->same_cells) {
             CK(cudaMemcpy(chi, chi_s, sizeof(double2) * nT * ns, cudaMemcpyDeviceToDevice));
         } else if (ns > 1) {
-            chi_kernel<<<dim3(nblk(nT, 128), ns - 1), 128, 0, st>>>(dg, 1, ns, pr->d_G[0], pr->d_G[1], pr->d_G[2],
+            chi_kernel<<<dim3(nblk(nT, 64), ns - 1), 64, 0, st>>>(dg, 1, ns, pr->d_G[0], pr->d_G[1], pr->d_G[2],
                                                                      pr->NT[0], pr->NT[1], pr->NT[2], 0, P.softening,
                                                                      P.sigma, chi);
             CK(cudaGetLastError());
@@ -1375,7 +1378,7 @@ extern "C" int qd_tables_build_dev(struct qd_problem *pr) {
         CK(cudaStreamSynchronize(st));
         qd_pool_free(work, 0);
     } else if (ns > 1) {
-        chi_kernel<<<dim3(nblk(nT, 128), ns - 1), 128, 0, st>>>(dg, 1, ns, pr->d_G[0], pr->d_G[1], pr->d_G[2],
+        chi_kernel<<<dim3(nblk(nT, 64), ns - 1), 64, 0, st>>>(dg, 1, ns, pr->d_G[0], pr->d_G[1], pr->d_G[2],
                                                                  pr->NT[0], pr->NT[1], pr->NT[2], 0, P.softening,
                                                                  P.sigma, chi);
         CK(cudaGetLastError());

@@ -173,14 +173,17 @@ class DeviceBuffer:
     """Owned device allocation."""
 
     def __init__(self, nbytes):
-        self.ptr = vp()
-        check(lib.qd_dev_alloc(int(nbytes), C.byref(self.ptr)))
+        self._free = lib.qd_dev_free  # held: module globals may be gone when collected at exit
+        self.ptr = None
+        p = vp()
+        check(lib.qd_dev_alloc(int(nbytes), C.byref(p)))
+        self.ptr = p
         self.nbytes = int(nbytes)
 
     def free(self):
-        if self.ptr:
-            lib.qd_dev_free(self.ptr)
-            self.ptr = vp()
+        p, self.ptr = getattr(self, "ptr", None), None
+        if p:
+            self._free(p)
 
     def __del__(self):
         self.free()
@@ -198,6 +201,7 @@ class DeviceBuffer:
 
 class Event:
     def __init__(self):
+        self._destroy = lib.qd_event_destroy  # held: module globals may be gone when collected at exit
         self.ev = vp()
         check(lib.qd_event_create(C.byref(self.ev)))
 
@@ -210,8 +214,9 @@ class Event:
         return float(ms.value)
 
     def __del__(self):
-        if self.ev:
-            lib.qd_event_destroy(self.ev)
+        ev, self.ev = getattr(self, "ev", None), None
+        if ev:
+            self._destroy(ev)
 
 
 def stage1_profile():

@@ -4,6 +4,7 @@ the command that the committed ncu summaries under profiles/ were captured
 from.
 
     python -m qudos_b200.profile_solve [--deck molecule_15] [--mg 7] [--prec mixed|fp64] [--solves 1] [--post]
+    python -m qudos_b200.profile_solve --gradients-c4
 
 One solve = H assembly (FP64, lower triangle) + the windowed eigensolve on
 the device.  With QD_PROFILE=1 in the environment the dense->band reduction
@@ -30,6 +31,31 @@ STAGES = ["assembly", "band reduction", "bulge chasing", "bisection", "inverse i
 STEPS = ["panel refresh", "panel QR", "T and VT", "X = A22 VT", "corrections", "W", "append", "trailing update"]
 
 
+def gradients_c4():
+    """The C4 gradient call alone: the 11^3 pyramid deck with 8 + 8 window
+    states, one FP64 solve, three warm calls of eigen_gradients_8_band for dot
+    height, base width, composition, field, Ep and gamma_1, then one more
+    call between cudaProfilerStart and cudaProfilerStop, so that
+    `ncu --profile-from-start off` lists the launches of that call only."""
+    import torch
+    params = [(L.QD_GRAD_LENGTH, 1, 4), (L.QD_GRAD_BASE, 1, 0), (L.QD_GRAD_COMPOSITION, 1, 0),
+              (L.QD_GRAD_FIELD, 0, 2), (L.QD_GRAD_EP, 0, 0), (L.QD_GRAD_GAMMA1, 0, 0)]
+    with tempfile.TemporaryDirectory() as d:
+        configs.write_deck(d, *configs.pyramid_11(mg=5, n_states=4, cme=0))
+        pr = q.Problem(d)
+        w, v = pr.solve(q.QD_PREC_FP64)
+    for rep in range(3):
+        t0 = time.perf_counter()
+        pr.gradients(v, params)
+        print("gradients, warm-up call %d: %.1f ms wall" % (rep, (time.perf_counter() - t0) * 1e3), flush=True)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    t0 = time.perf_counter()
+    pr.gradients(v, params)
+    print("gradients, listed call: %.1f ms wall" % ((time.perf_counter() - t0) * 1e3), flush=True)
+    torch.cuda.cudart().cudaProfilerStop()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--mg", type=int, default=7)
@@ -39,7 +65,12 @@ def main(argv=None):
     ap.add_argument("--deck", choices=["molecule_15", "lens_7", "pyramid_11"], default="molecule_15")
     ap.add_argument("--xprod-curve", action="store_true",
                     help="print the X-product kernel's bandwidth per launch of the last solve, binned by m")
+    ap.add_argument("--gradients-c4", action="store_true",
+                    help="run only the C4 gradient call (profiled region: one warm call)")
     a = ap.parse_args(argv)
+    if a.gradients_c4:
+        gradients_c4()
+        return
     with tempfile.TemporaryDirectory() as d:
         if a.deck == "molecule_15":
             deck = configs.molecule_15(mg=a.mg, cme=4 if a.post else 0)

@@ -22,6 +22,9 @@ class Problem:
         """Loads parameters.in / supercell.in from directory.  tuned: put the
         package's autotuner cache into the library's tuning table (once per
         process) before the first solve."""
+        # held on the instance: a Problem collected at interpreter exit may
+        # find this module's globals already cleared
+        self._free = L.lib.qd_problem_free
         if tuned:
             from . import autotune
             autotune.ensure_loaded()
@@ -38,9 +41,9 @@ class Problem:
         self.n_shape = L.lib.qd_problem_n_shape(self._h)
 
     def close(self):
-        if self._h:
-            L.lib.qd_problem_free(self._h)
-            self._h = C.c_void_p()
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._free(h)
 
     def __del__(self):
         self.close()
