@@ -135,3 +135,54 @@ def test_tuning_table_and_cache(tmp_path):
         assert autotune.load(str(tmp_path / "absent.json")) == 0
     finally:
         autotune.load()
+
+
+@pytest.mark.parametrize("name", ["molecule", "all_shapes"])
+def test_material_tangents_match_central_differences(name, tmp_path):
+    """qd_material_tangent, the exact d(material parameters)/d(scale) behind the
+    Ep and gamma_1 gradients, against central differences of the host material
+    function in the scale of the binary table's Ep and gamma_1 columns
+    (qd_scale_Ep, qd_scale_gL1); every field that the scale does not move must
+    have a zero tangent."""
+    d = cases.CASES[name](2, tmp_path)
+    p, _ = inputs.load(d)
+    pr = q.Problem(d)
+    ns = pr.n_shape
+    geo = (L.SupercellGeometry * ns)()
+    L.check(L.lib.qd_problem_geometry(pr.handle, geo, ns))
+    mat_fn = L.lib.qd_material_parameters
+    mat_fn.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    tan_fn = L.lib.qd_material_tangent
+    tan_fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    scales = {0: ctypes.c_double.in_dll(L.lib, "qd_scale_Ep"), 1: ctypes.c_double.in_dll(L.lib, "qd_scale_gL1")}
+    fields = [f for f, _ in L.MaterialParams._fields_]
+
+    def mats(which=None, scale=1.0):
+        out = (L.MaterialParams * ns)()
+        if which is not None:
+            scales[which].value = scale
+        try:
+            L.check(mat_fn(p["T"], p["Piezo"], ns, ctypes.addressof(geo), ctypes.addressof(out)))
+        finally:
+            scales[0].value = scales[1].value = 1.0
+        return out
+
+    base = mats()
+    ref = pr.materials(ns)  # the problem's own materials: same function, same inputs
+    for s in range(ns):
+        for f in fields:
+            assert getattr(base[s], f) == ref[s][f], (s, f)
+    h = 1e-5
+    for which in (0, 1):
+        dm = (L.MaterialParams * ns)()
+        L.check(tan_fn(which, ns, ctypes.addressof(geo), ctypes.addressof(base), ctypes.addressof(dm)))
+        plus, minus = mats(which, 1.0 + h), mats(which, 1.0 - h)
+        moved = 0
+        for s in range(ns):
+            for f in fields:
+                fd = (getattr(plus[s], f) - getattr(minus[s], f)) / (2 * h)
+                ex = getattr(dm[s], f)
+                scale = max(abs(getattr(base[s], f)), 1e-3)
+                assert abs(fd - ex) <= 1e-7 * scale, (which, s, f, fd, ex)
+                moved += ex != 0.0
+        assert moved > 0
